@@ -1,0 +1,268 @@
+// gcdt.cu -- CUDA kernels, the device launch backend and the C ABI.
+#include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "solver.cuh"
+#include "../../include/gcdt.h"
+
+namespace gcdt {
+
+constexpr int kBlock = 256;
+
+#define GCDT_KERNEL(name, body)                                            \
+    __global__ void __launch_bounds__(kBlock) name(Ctx c, int n) {         \
+        int i = blockIdx.x * kBlock + threadIdx.x;                         \
+        if (i < n) body(c, i);                                             \
+    }
+
+GCDT_KERNEL(gcdt_keys, body_keys)
+GCDT_KERNEL(gcdt_gather, body_gather)
+GCDT_KERNEL(gcdt_root, body_root)
+GCDT_KERNEL(gcdt_initloc, body_initloc)
+GCDT_KERNEL(gcdt_reloc_vote, body_reloc_vote)
+GCDT_KERNEL(gcdt_split, body_split)
+GCDT_KERNEL(gcdt_fix, body_fix)
+GCDT_KERNEL(gcdt_flip_check, body_flip_check)
+GCDT_KERNEL(gcdt_flip_do, body_flip_do)
+GCDT_KERNEL(gcdt_flip_fix, body_flip_fix)
+GCDT_KERNEL(gcdt_output, body_output)
+GCDT_KERNEL(gcdt_vt, body_vt)
+GCDT_KERNEL(gcdt_seg_init, body_seg_init)
+GCDT_KERNEL(gcdt_cwalk, body_cwalk)
+GCDT_KERNEL(gcdt_cclaim, body_cclaim)
+GCDT_KERNEL(gcdt_cproc, body_cproc)
+
+__global__ void gcdt_predicates(const int2* q, int n, int* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int2 a = q[4 * i], b = q[4 * i + 1], cc = q[4 * i + 2], d = q[4 * i + 3];
+    out[3 * i] = orient2d(a, b, cc);
+    out[3 * i + 1] = incircle(a, b, cc, d);
+    out[3 * i + 2] = incircle_sos(a, b, cc, d);
+}
+
+constexpr int ST_CUDA = 32;
+
+struct DeviceBackend {
+    cudaStream_t st = nullptr;
+    Counters* dcnt = nullptr;
+    Counters* hcnt = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_bytes = 0;
+    cudaError_t err = cudaSuccess;
+    long long launches = 0;
+
+    void note(cudaError_t e) { if (e != cudaSuccess && err == cudaSuccess) err = e; }
+
+    void launch(int k, const Ctx& c, long long n) {
+        if (n <= 0 || err != cudaSuccess) return;
+        unsigned grid = (unsigned)((n + kBlock - 1) / kBlock);
+        int nn = (int)n;
+        switch (k) {
+        case K_KEYS: gcdt_keys<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_GATHER: gcdt_gather<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_ROOT: gcdt_root<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_INITLOC: gcdt_initloc<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_RELOC_VOTE: gcdt_reloc_vote<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_SPLIT: gcdt_split<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_FIX: gcdt_fix<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_FLIP_CHECK: gcdt_flip_check<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_FLIP_DO: gcdt_flip_do<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_FLIP_FIX: gcdt_flip_fix<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_OUTPUT: gcdt_output<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_VT: gcdt_vt<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_SEG_INIT: gcdt_seg_init<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_CWALK: gcdt_cwalk<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_CCLAIM: gcdt_cclaim<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_CPROC: gcdt_cproc<<<grid, kBlock, 0, st>>>(c, nn); break;
+        default: break;
+        }
+        launches++;
+        note(cudaGetLastError());
+    }
+    void fill(void* p, int v, size_t bytes) { note(cudaMemsetAsync(p, v, bytes, st)); }
+    void reset_lists() { note(cudaMemsetAsync(&dcnt->n_next, 0, 3 * sizeof(int), st)); }
+    void set_scratch_top(int) { note(cudaMemsetAsync(&dcnt->scratch_top, 0, sizeof(int), st)); }
+    void read(Counters* h) {
+        note(cudaMemcpyAsync(hcnt, dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        note(cudaStreamSynchronize(st));
+        *h = *hcnt;
+        if (err != cudaSuccess) h->status |= ST_CUDA;
+    }
+    void sort(Ctx& c, int n) {
+        cub::DoubleBuffer<unsigned long long> dk(c.keys, c.keys_alt);
+        cub::DoubleBuffer<int> dv(c.vals, c.vals_alt);
+        size_t bytes = sort_bytes;
+        note(cub::DeviceRadixSort::SortPairs(sort_tmp, bytes, dk, dv, n, 0, 60, st));
+        c.keys = dk.Current(); c.keys_alt = dk.Alternate();
+        c.vals = dv.Current(); c.vals_alt = dv.Alternate();
+    }
+};
+
+inline size_t sort_temp_bytes(int64_t n) {
+    if (n <= 0) return 0;
+    cub::DoubleBuffer<unsigned long long> dk(nullptr, nullptr);
+    cub::DoubleBuffer<int> dv(nullptr, nullptr);
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, (int)n, 0, 60);
+    return bytes;
+}
+
+inline gcdt_status map_status(int bits) {
+    if (bits == 0) return GCDT_OK;
+    if (bits & ST_CUDA) return GCDT_CUDA_ERROR;
+    if (bits & ST_BAD_INPUT) return GCDT_BAD_INPUT;
+    if (bits & ST_CONSTRAINT_FAIL) return GCDT_CONSTRAINT_FAIL;
+    if (bits & ST_ITER_LIMIT) return GCDT_ITER_LIMIT;
+    if (bits & ST_OOM) return GCDT_OOM;
+    return GCDT_INTERNAL;
+}
+
+}  // namespace gcdt
+
+using namespace gcdt;
+
+struct gcdt_context {
+    int device = 0;
+    int64_t max_n = 0, max_s = 0;
+    size_t arena_bytes = 0;
+    char* arena = nullptr;
+    Counters* hcnt = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    gcdt_stats stats{};
+};
+
+namespace {
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+}  // namespace
+
+extern "C" size_t gcdt_workspace_bytes(int64_t n, int64_t s) {
+    if (n < 0 || s < 0 || n > GCDT_MAX_POINTS) return 0;
+    return make_plan(n, s, sort_temp_bytes(n)).L.total;
+}
+
+extern "C" gcdt_status gcdt_create(gcdt_context** out, int device, int64_t max_points, int64_t max_segments) {
+    if (!out) return GCDT_BAD_INPUT;
+    *out = nullptr;
+    if (max_points < 0 || max_points > GCDT_MAX_POINTS || max_segments < 0 || max_segments > (int64_t(1) << 30))
+        return GCDT_BAD_INPUT;
+    gcdt_context* ctx = new (std::nothrow) gcdt_context();
+    if (!ctx) return GCDT_OOM;
+    ctx->device = device;
+    ctx->max_n = max_points;
+    ctx->max_s = max_segments;
+    DeviceGuard g(device);
+    ctx->arena_bytes = gcdt_workspace_bytes(max_points, max_segments);
+    if (cudaMalloc(&ctx->arena, ctx->arena_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return GCDT_OOM;
+    }
+    if (cudaMallocHost(&ctx->hcnt, sizeof(Counters)) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        gcdt_destroy(ctx);
+        return GCDT_CUDA_ERROR;
+    }
+    *out = ctx;
+    return GCDT_OK;
+}
+
+extern "C" void gcdt_destroy(gcdt_context* ctx) {
+    if (!ctx) return;
+    DeviceGuard g(ctx->device);
+    if (ctx->arena) cudaFree(ctx->arena);
+    if (ctx->hcnt) cudaFreeHost(ctx->hcnt);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    delete ctx;
+}
+
+extern "C" gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_points, int32_t n,
+                                        const int32_t* d_segments, int32_t s,
+                                        int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                        int32_t* n_tris, void* stream) {
+    if (!ctx || n < 0 || s < 0 || (n > 0 && !d_points) || (s > 0 && !d_segments) ||
+        !d_tris || !d_adj || !d_cflags)
+        return GCDT_BAD_INPUT;
+    if (n > ctx->max_n || s > ctx->max_s) return GCDT_OOM;
+    DeviceGuard g(ctx->device);
+    Plan plan = make_plan(n, s, sort_temp_bytes(n));
+    if (plan.L.total > ctx->arena_bytes) return GCDT_OOM;
+    Ctx c = bind_ctx(ctx->arena, plan);
+    c.in_xy = reinterpret_cast<const int2*>(d_points);
+    c.in_cons = reinterpret_cast<const int2*>(d_segments);
+    c.out_tris = d_tris;
+    c.out_adj = d_adj;
+    c.out_cflags = d_cflags;
+    DeviceBackend bk;
+    bk.st = static_cast<cudaStream_t>(stream);
+    bk.dcnt = c.cnt;
+    bk.hcnt = ctx->hcnt;
+    bk.sort_tmp = ctx->arena + plan.o_sort_tmp;
+    bk.sort_bytes = plan.sort_temp_bytes;
+    SolveStats st;
+    cudaEventRecord(ctx->ev0, bk.st);
+    int bits = run_solve(bk, c, st);
+    cudaEventRecord(ctx->ev1, bk.st);
+    bk.note(cudaEventSynchronize(ctx->ev1));
+    if (bk.err != cudaSuccess) bits |= ST_CUDA;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    gcdt_stats& S = ctx->stats;
+    S.n_points = n;
+    S.n_segments = s;
+    S.n_triangles = 2 * (int64_t)n + 2;
+    S.insertion_rounds = st.rounds;
+    S.flip_subrounds = st.flip_subrounds;
+    S.flips = st.flips;
+    S.constraint_rounds = st.constraint_rounds;
+    S.host_syncs = st.host_syncs;
+    S.kernel_launches = bk.launches;
+    S.device_ms = ms;
+    gcdt_status rc = map_status(bits);
+    if (rc == GCDT_OK && n_tris) *n_tris = 2 * n + 2;
+    return rc;
+}
+
+extern "C" gcdt_status gcdt_get_stats(const gcdt_context* ctx, gcdt_stats* out) {
+    if (!ctx || !out) return GCDT_BAD_INPUT;
+    *out = ctx->stats;
+    return GCDT_OK;
+}
+
+extern "C" const char* gcdt_status_string(gcdt_status s) {
+    switch (s) {
+    case GCDT_OK: return "ok";
+    case GCDT_BAD_INPUT: return "bad input (coordinate range, duplicate point or bad segment)";
+    case GCDT_OOM: return "problem larger than the context";
+    case GCDT_ITER_LIMIT: return "iteration limit reached";
+    case GCDT_CONSTRAINT_FAIL: return "constraint segments cross";
+    case GCDT_CUDA_ERROR: return "CUDA error";
+    case GCDT_INTERNAL: return "internal error";
+    }
+    return "unknown status";
+}
+
+extern "C" gcdt_status gcdt_eval_predicates(const int32_t* d_quads, int32_t n_cases, int32_t* d_out, void* stream) {
+    if (n_cases < 0 || (n_cases > 0 && (!d_quads || !d_out))) return GCDT_BAD_INPUT;
+    if (n_cases == 0) return GCDT_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    gcdt_predicates<<<(n_cases + 255) / 256, 256, 0, st>>>(reinterpret_cast<const int2*>(d_quads), n_cases, d_out);
+    if (cudaGetLastError() != cudaSuccess) return GCDT_CUDA_ERROR;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return GCDT_CUDA_ERROR;
+    return GCDT_OK;
+}

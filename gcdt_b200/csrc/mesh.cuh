@@ -1,0 +1,762 @@
+// mesh.cuh -- data layout and per-element bodies of every kernel of the
+// CDT path.  The bodies are __host__ __device__ so that the same code is
+// what the CUDA kernels (kernels.cu) run, one body call per thread.
+//
+// Layout in HBM (structure of arrays, one row per point or triangle):
+//   P[v]      int2   point v in Morton-sorted order; corners at N..N+3
+//   perm[v]   int    input index of sorted point v (corners map to N+k)
+//   TV[t]     int4   (v0, v1, v2, cflags) -- CCW vertices, bit k of .w set when
+//                    the edge opposite v_k is a constraint edge
+//   TA[t]     int4   (a0, a1, a2, -)  a_k = 4*n + j: neighbour n across the
+//                    edge opposite v_k, which is opposite slot j in n; -1 = box
+// Triangle slots never move: the two root triangles are 0 and 1, and sorted
+// point q creates exactly two new slots, 2+2q and 3+2q, when it is inserted
+// (1->3 split of one triangle, or 2->4 split of the two triangles sharing the
+// edge q lies on).  The final mesh therefore has exactly 2N+2 triangles
+// (reference count T = 2N+2 with the 4 box corners).
+//
+// Reference conventions kept (yingtix/gCDT): int2 points at 30-bit resolution
+// (include/math_base.cuh:19-29), box corners (0,0),(R,0),(R,R),(0,R) at
+// N..N+3 and root triangles (N,N+1,N+3),(N+1,N+2,N+3) (rawMesh.cu:5-22), CCW
+// triangles whose adj.x is the neighbour across the edge opposite .x
+// (rawMesh.cu:269-276), flips iff inCircle > 0 (kernel.cu:2218-2219) and
+// constraint edges never flipped (kernel.cu:2203-2205).
+#pragma once
+#include <cstdint>
+#include "predicates.cuh"
+
+#if defined(__CUDACC__)
+#include <cooperative_groups.h>
+#endif
+
+#define GCDT_HD __host__ __device__ __forceinline__
+
+namespace gcdt {
+
+constexpr int kBoxMax = (1 << 30) - 1;   // R = 2^30 - 1
+
+enum StatusBits : int {
+    ST_OK = 0,
+    ST_BAD_INPUT = 1,
+    ST_OOM = 2,
+    ST_ITER_LIMIT = 4,
+    ST_CONSTRAINT_FAIL = 8,
+    ST_INTERNAL = 16,
+};
+
+// Device-resident counters; one 128-byte line.
+struct Counters {
+    int status;          // OR of StatusBits
+    int n_next;          // size of the list being appended to
+    int n_win;           // points inserted this round
+    int n_flip;          // flips performed this sub-round
+    int scratch_top;     // bump allocator of the constraint scratch
+    int n_done;          // segments finished this round
+    int n_lawson;        // triangles queued for the constrained flip pass
+    int pad1;
+    unsigned long long flips_total;
+    unsigned long long walk_steps;
+    unsigned long long pad2[4];
+};
+
+struct Ctx {
+    int n;          // input points
+    int s;          // input segments
+    int ntri;       // 2n + 2
+    unsigned round; // insertion round / epoch stamp
+    unsigned sr;    // flip sub-round stamp (monotone over the whole solve)
+    unsigned lawson_sr;  // queue stamp of the constrained flip pass
+    int list_n;     // length of the list a launch iterates over
+
+    const int2* in_xy;
+    const int2* in_cons;
+
+    unsigned long long* keys;
+    unsigned long long* keys_alt;
+    int* vals;
+    int* vals_alt;
+
+    int2* P;
+    int* perm;
+    int* rank;
+
+    int4* TV;
+    int4* TA;
+
+    int* loc;                 // triangle holding an uninserted point, -1 once inserted
+    signed char* pedge;       // slot of the edge the point lies on, -1 inside
+    int* act;                 // active point list (read)
+    int* act_next;            // active point list (append)
+    unsigned long long* vote; // per triangle: (round<<32) | ~hash(point)
+    int2* ins;                // per triangle: (round, 8*q + split code)
+    int* modR;                // per triangle: last round it changed
+    int2* winners;            // (q, t) inserted this round
+
+    unsigned long long* claim;  // per triangle: (stamp<<32) | ~key
+    int2* cand;                 // per queue entry: (4t+i, 4n+j) or (-1,-1)
+    int4* fmap;                 // per flipped triangle: old slot -> new (4t+s)
+    int* fst;                   // per triangle: sub-round it was flipped
+    int* qst;                   // per triangle: queue stamp (dedup)
+    int* queue;                 // flip queue (read)
+    int* queue_next;            // flip queue (append)
+    int* flipped;               // flips of this sub-round (t of each pair)
+
+    int4* seg;          // per segment: (a, b, stop, -)  sorted ids; a advances
+    int* pend;          // pending segment list (read)
+    int* pend_next;     // pending segment list (append)
+    int4* pinfo;        // per pending entry: (start 4t+i, ncross, scratch base, ring size | -1)
+    int* scratch;       // constraint scratch
+    int scratch_cap;
+    int* vt;            // vertex -> incident triangle
+    int* lq;            // triangles queued for the constrained flip pass
+
+    int* out_tris;
+    int* out_adj;
+    unsigned char* out_cflags;
+
+    Counters* cnt;
+};
+
+// ---------------------------------------------------------------- helpers
+
+GCDT_HD int enc(int t, int s) { return (t << 2) | s; }
+GCDT_HD int nx3(int i) { return i == 2 ? 0 : i + 1; }
+GCDT_HD int pv3(int i) { return i == 0 ? 2 : i - 1; }
+GCDT_HD int comp(const int4& v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+GCDT_HD void setc(int4& v, int i, int x) {
+    if (i == 0) v.x = x; else if (i == 1) v.y = x; else v.z = x;
+}
+GCDT_HD int slot_of(const int4& tv, int v) { return tv.x == v ? 0 : (tv.y == v ? 1 : 2); }
+
+GCDT_HD uint32_t hash32(uint32_t x) {  // bijective 32-bit mix
+    x ^= x >> 16; x *= 0x7feb352dU;
+    x ^= x >> 15; x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+GCDT_HD unsigned long long at_max64(unsigned long long* p, unsigned long long v) {
+#if defined(__CUDA_ARCH__)
+    return atomicMax(p, v);
+#else
+    unsigned long long o = *p; if (v > o) *p = v; return o;
+#endif
+}
+GCDT_HD int at_add(int* p, int v) {
+#if defined(__CUDA_ARCH__)
+    return atomicAdd(p, v);
+#else
+    int o = *p; *p = o + v; return o;
+#endif
+}
+GCDT_HD unsigned long long at_add64(unsigned long long* p, unsigned long long v) {
+#if defined(__CUDA_ARCH__)
+    return atomicAdd(p, v);
+#else
+    unsigned long long o = *p; *p = o + v; return o;
+#endif
+}
+GCDT_HD int at_exch(int* p, int v) {
+#if defined(__CUDA_ARCH__)
+    return atomicExch(p, v);
+#else
+    int o = *p; *p = v; return o;
+#endif
+}
+GCDT_HD int at_or(int* p, int v) {
+#if defined(__CUDA_ARCH__)
+    return atomicOr(p, v);
+#else
+    int o = *p; *p = o | v; return o;
+#endif
+}
+GCDT_HD void fail(const Ctx& c, int bits) { at_or(&c.cnt->status, bits); }
+
+// Append one element to a list whose length lives at *ctr.  On the GPU the
+// threads of a warp that append together take one atomic between them.
+GCDT_HD int append_slot(int* ctr) {
+#if defined(__CUDA_ARCH__)
+    namespace cg = cooperative_groups;
+    cg::coalesced_group g = cg::coalesced_threads();
+    int base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(ctr, (int)g.size());
+    base = g.shfl(base, 0);
+    return base + (int)g.thread_rank();
+#else
+    int o = *ctr; *ctr = o + 1; return o;
+#endif
+}
+
+GCDT_HD unsigned long long morton60(int2 p) {
+    unsigned long long x = (unsigned)p.x, y = (unsigned)p.y;
+    auto spread = [](unsigned long long v) {
+        v &= 0x3fffffffULL;
+        v = (v | (v << 16)) & 0x0000FFFF0000FFFFULL;
+        v = (v | (v << 8)) & 0x00FF00FF00FF00FFULL;
+        v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0FULL;
+        v = (v | (v << 2)) & 0x3333333333333333ULL;
+        v = (v | (v << 1)) & 0x5555555555555555ULL;
+        return v;
+    };
+    return spread(x) | (spread(y) << 1);
+}
+
+// ---------------------------------------------------------------- set-up
+
+// One thread per input point: Morton key + range check.
+GCDT_HD void body_keys(const Ctx& c, int i) {
+    int2 p = c.in_xy[i];
+    if (p.x < 1 || p.y < 1 || p.x > kBoxMax - 1 || p.y > kBoxMax - 1) fail(c, ST_BAD_INPUT);
+    c.keys[i] = morton60(p);
+    c.vals[i] = i;
+}
+
+// After the sort (sorted keys/vals in keys/vals): gather points, permutation,
+// inverse permutation; adjacent equal keys are duplicate points.
+GCDT_HD void body_gather(const Ctx& c, int i) {
+    if (i < c.n) {
+        int j = c.vals[i];
+        c.P[i] = c.in_xy[j];
+        c.perm[i] = j;
+        c.rank[j] = i;
+        if (i > 0 && c.keys[i] == c.keys[i - 1]) fail(c, ST_BAD_INPUT);
+        c.loc[i] = 0;
+        c.act[i] = i;
+    } else if (i < c.n + 4) {
+        int k = i - c.n;
+        int2 corner;
+        corner.x = (k == 1 || k == 2) ? kBoxMax : 0;
+        corner.y = (k >= 2) ? kBoxMax : 0;
+        c.P[i] = corner;
+        c.perm[i] = i;
+    }
+}
+
+// Root triangles (rawMesh.cu:16-21) -- one thread.
+GCDT_HD void body_root(const Ctx& c, int) {
+    int n = c.n;
+    c.TV[0] = make_int4(n, n + 1, n + 3, 0);
+    c.TV[1] = make_int4(n + 1, n + 2, n + 3, 0);
+    c.TA[0] = make_int4(enc(1, 1), -1, -1, 0);
+    c.TA[1] = make_int4(-1, enc(0, 0), -1, 0);
+}
+
+// Root triangle of each point: orient against the diagonal (R,0)-(0,R)
+// (rawMesh.cu:37-57); a point on the diagonal is in the closed triangle 0.
+GCDT_HD void body_initloc(const Ctx& c, int i) {
+    int2 rd = make_int2(kBoxMax, 0), lt = make_int2(0, kBoxMax);
+    c.loc[i] = orient2d(rd, lt, c.P[i]) >= 0 ? 0 : 1;
+}
+
+// ---------------------------------------------------------------- insertion
+
+// Visibility walk from t to the triangle whose closed interior holds p.
+// Terminates in a Delaunay triangulation (acyclic in-front-of relation).
+GCDT_HD int walk(const Ctx& c, int t, int2 p, int limit, int* steps) {
+    for (int it = 0; it < limit; ++it) {
+        int4 tv = c.TV[t];
+        int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
+        int side = -1;
+        int r = it % 3;
+        for (int k = 0; k < 3 && side < 0; ++k) {
+            int s = r + k; if (s >= 3) s -= 3;
+            int o = s == 0 ? orient2d(b, cc, p) : (s == 1 ? orient2d(cc, a, p) : orient2d(a, b, p));
+            if (o < 0) side = s;
+        }
+        if (side < 0) { *steps += it; return t; }
+        int nb = comp(c.TA[t], side);
+        if (nb < 0) { *steps += it; return -1; }
+        t = nb >> 2;
+    }
+    *steps += limit;
+    return -1;
+}
+
+// Active point: relocate if its triangle changed in the previous round,
+// keep it in the next list, and vote for the triangle(s) it will split.
+// Winner per triangle = minimum hash32(q): random insertion order per
+// triangle, independent of thread scheduling.
+GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
+    int q = c.act[k];
+    int t = c.loc[q];
+    if (t < 0) return;                       // inserted last round
+    int2 p = c.P[q];
+    if (c.modR[t] == (int)c.round - 1) {
+        int steps = 0;
+        int nt = walk(c, t, p, 1 << 20, &steps);
+        if (nt < 0) { fail(c, ST_ITER_LIMIT); return; }
+        t = nt;
+        c.loc[q] = t;
+    }
+    c.act_next[append_slot(&c.cnt->n_next)] = q;
+    int4 tv = c.TV[t];
+    int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
+    int o0 = orient2d(b, cc, p), o1 = orient2d(cc, a, p), o2 = orient2d(a, b, p);
+    int e = o0 == 0 ? 0 : (o1 == 0 ? 1 : (o2 == 0 ? 2 : -1));
+    if (o0 < 0 || o1 < 0 || o2 < 0) fail(c, ST_INTERNAL);
+    c.pedge[q] = (signed char)e;
+    unsigned long long key = ((unsigned long long)c.round << 32) | (0xffffffffu - hash32((uint32_t)q));
+    if (c.vote[t] < key) at_max64(&c.vote[t], key);
+    if (e >= 0) {
+        int n = comp(c.TA[t], e) >> 2;
+        if (c.vote[n] < key) at_max64(&c.vote[n], key);
+    }
+}
+
+// Winners split their triangle(s).  Child j of a split triangle is the
+// triangle with vertex j replaced by q; it keeps the old edge j in slot j.
+// Outer adjacency is written as the old neighbour and resolved in body_fix.
+GCDT_HD void body_split(const Ctx& c, int k) {
+    int q = c.act[k];
+    int t = c.loc[q];
+    unsigned long long key = ((unsigned long long)c.round << 32) | (0xffffffffu - hash32((uint32_t)q));
+    if (c.vote[t] != key) return;
+    int e = c.pedge[q];
+    int T1 = 2 + 2 * q, T2 = 3 + 2 * q;
+    int4 tv = c.TV[t], ta = c.TA[t];
+    int fl = tv.w;
+    if (e < 0) {
+        int ch[3] = {t, T1, T2};
+        for (int j = 0; j < 3; ++j) {
+            int4 v = tv; setc(v, j, q); v.w = fl & (1 << j);
+            int4 a;
+            a.w = 0;
+            for (int kk = 0; kk < 3; ++kk)
+                setc(a, kk, kk == j ? comp(ta, j) : enc(ch[kk], j));
+            c.TV[ch[j]] = v;
+            c.TA[ch[j]] = a;
+        }
+        c.ins[t] = make_int2((int)c.round, q * 8 + 7);
+        c.modR[t] = (int)c.round;
+    } else {
+        int en = comp(ta, e);
+        int n = en >> 2, e2 = en & 3;
+        if (c.vote[n] != key) return;
+        int4 nv = c.TV[n], na = c.TA[n];
+        int gl = nv.w;
+        // children: A1 = child_{e+1}(t) -> t, A2 = child_{e+2}(t) -> T1,
+        //           B1 = child_{e2+1}(n) -> n, B2 = child_{e2+2}(n) -> T2
+        int e1 = nx3(e), e_2 = nx3(e1), f1 = nx3(e2), f2 = nx3(f1);
+        int A1 = t, A2 = T1, B1 = n, B2 = T2;
+        int4 v, a;
+        // A1
+        v = tv; setc(v, e1, q); v.w = fl & ((1 << e1) | (1 << e));
+        a = make_int4(0, 0, 0, 0);
+        setc(a, e1, comp(ta, e1)); setc(a, e_2, enc(A2, e1)); setc(a, e, enc(B2, e2));
+        c.TV[A1] = v; c.TA[A1] = a;
+        // A2
+        v = tv; setc(v, e_2, q); v.w = fl & ((1 << e_2) | (1 << e));
+        a = make_int4(0, 0, 0, 0);
+        setc(a, e_2, comp(ta, e_2)); setc(a, e1, enc(A1, e_2)); setc(a, e, enc(B1, e2));
+        c.TV[A2] = v; c.TA[A2] = a;
+        // B1
+        v = nv; setc(v, f1, q); v.w = gl & ((1 << f1) | (1 << e2));
+        a = make_int4(0, 0, 0, 0);
+        setc(a, f1, comp(na, f1)); setc(a, f2, enc(B2, f1)); setc(a, e2, enc(A2, e));
+        c.TV[B1] = v; c.TA[B1] = a;
+        // B2
+        v = nv; setc(v, f2, q); v.w = gl & ((1 << f2) | (1 << e2));
+        a = make_int4(0, 0, 0, 0);
+        setc(a, f2, comp(na, f2)); setc(a, f1, enc(B1, f2)); setc(a, e2, enc(A1, e));
+        c.TV[B2] = v; c.TA[B2] = a;
+        c.ins[t] = make_int2((int)c.round, q * 8 + e);
+        c.ins[n] = make_int2((int)c.round, q * 8 + 3 + e2);
+        c.modR[t] = (int)c.round;
+        c.modR[n] = (int)c.round;
+    }
+    c.loc[q] = -1;
+    c.winners[append_slot(&c.cnt->n_win)] = make_int2(q, t);
+}
+
+// Child of triangle m (split this round) that now holds m's old edge `ms`.
+GCDT_HD int split_child(int2 im, int m, int ms) {
+    int code = im.y & 7, qm = im.y >> 3;
+    if (code == 7) return ms == 0 ? m : (ms == 1 ? 2 + 2 * qm : 3 + 2 * qm);
+    if (code < 3) return ms == nx3(code) ? m : 2 + 2 * qm;
+    int e = code - 3;
+    return ms == nx3(e) ? m : 3 + 2 * qm;
+}
+
+GCDT_HD void push_queue(const Ctx& c, int t) {
+    if (at_exch(&c.qst[t], (int)c.sr) != (int)c.sr)
+        c.queue_next[append_slot(&c.cnt->n_next)] = t;
+}
+
+GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
+    int4* row = &c.TA[ch];
+    int old = comp(*row, s);
+    if (old < 0) return;
+    int m = old >> 2, ms = old & 3;
+    int2 im = c.ins[m];
+    if (im.x == (int)c.round) {
+        ((int*)row)[s] = enc(split_child(im, m, ms), ms);
+    } else {
+        ((int*)&c.TA[m])[ms] = enc(ch, s);
+    }
+}
+
+// Resolve outer adjacency of the children of one inserted point and queue
+// them for the flip phase (c.sr = first sub-round of this round).
+GCDT_HD void body_fix(const Ctx& c, int k) {
+    int2 w = c.winners[k];
+    int q = w.x, t = w.y;
+    int T1 = 2 + 2 * q, T2 = 3 + 2 * q;
+    int code = c.ins[t].y & 7;
+    if (code == 7) {
+        resolve_split_edge(c, t, 0);
+        resolve_split_edge(c, T1, 1);
+        resolve_split_edge(c, T2, 2);
+        push_queue(c, t); push_queue(c, T1); push_queue(c, T2);
+    } else {
+        int e = code;
+        int e1 = nx3(e), e_2 = nx3(e1);
+        int en = comp(c.TA[T1], e);     // A2 slot e = enc(B1, e2)
+        int n = en >> 2, e2 = en & 3;
+        int f1 = nx3(e2), f2 = nx3(f1);
+        resolve_split_edge(c, t, e1);
+        resolve_split_edge(c, T1, e_2);
+        resolve_split_edge(c, n, f1);
+        resolve_split_edge(c, T2, f2);
+        push_queue(c, t); push_queue(c, T1); push_queue(c, n); push_queue(c, T2);
+    }
+}
+
+// ---------------------------------------------------------------- flips
+
+// Queue entry t: find the first edge of t that is not locally Delaunay
+// (perturbed incircle > 0, not a constraint) and claim both triangles.
+// The claim priority hash32(4t+i) is unique (hash32 is a bijection); the
+// smallest wins both triangles (atomicMax of its complement), so conflicts
+// resolve like a random-priority independent set, whatever the schedule.
+GCDT_HD void body_flip_check(const Ctx& c, int k) {
+    int t = c.queue[k];
+    int4 tv = c.TV[t], ta = c.TA[t];
+    int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
+    for (int i = 0; i < 3; ++i) {
+        int en = comp(ta, i);
+        if (en < 0 || ((tv.w >> i) & 1)) continue;
+        int n = en >> 2, j = en & 3;
+        int d = comp(c.TV[n], j);
+        if (incircle_sos(a, b, cc, c.P[d]) > 0) {
+            int key = enc(t, i);
+            unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)key));
+            at_max64(&c.claim[t], ck);
+            at_max64(&c.claim[n], ck);
+            c.cand[k] = make_int2(key, en);
+            return;
+        }
+    }
+    c.cand[k] = make_int2(-1, -1);
+}
+
+// Winners flip: t=(A,B,C) with A in slot i, n=(D,C,B) with D in slot j
+// become t=(A,B,D), n=(A,D,C).  Losers are re-queued.
+GCDT_HD void body_flip_do(const Ctx& c, int k) {
+    int2 cd = c.cand[k];
+    if (cd.x < 0) return;
+    int t = cd.x >> 2, i = cd.x & 3;
+    int n = cd.y >> 2, j = cd.y & 3;
+    unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)cd.x));
+    if (c.claim[t] != ck || c.claim[n] != ck) {
+        // re-check next sub-round; stamp sr+1 is the next queue's stamp
+        if (at_exch(&c.qst[t], (int)c.sr + 1) != (int)c.sr + 1)
+            c.queue_next[append_slot(&c.cnt->n_next)] = t;
+        return;
+    }
+    int4 tv = c.TV[t], ta = c.TA[t], nv = c.TV[n], na = c.TA[n];
+    int i1 = nx3(i), i2 = nx3(i1), j1 = nx3(j), j2 = nx3(j1);
+    int A = comp(tv, i), B = comp(tv, i1), C = comp(tv, i2), D = comp(nv, j);
+    int ft = tv.w, fn = nv.w;
+    c.TV[t] = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
+    c.TA[t] = make_int4(comp(na, j1), enc(n, 2), comp(ta, i2), 0);
+    c.TV[n] = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
+    c.TA[n] = make_int4(comp(na, j2), comp(ta, i1), enc(t, 1), 0);
+    int4 mt = make_int4(-1, -1, -1, 0), mn = make_int4(-1, -1, -1, 0);
+    setc(mt, i1, enc(n, 1)); setc(mt, i2, enc(t, 2));
+    setc(mn, j1, enc(t, 0)); setc(mn, j2, enc(n, 0));
+    c.fmap[t] = mt;
+    c.fmap[n] = mn;
+    c.fst[t] = (int)c.sr;
+    c.fst[n] = (int)c.sr;
+    c.modR[t] = (int)c.round;
+    c.modR[n] = (int)c.round;
+    c.flipped[append_slot(&c.cnt->n_flip)] = t;
+    if (at_exch(&c.qst[t], (int)c.sr + 1) != (int)c.sr + 1)
+        c.queue_next[append_slot(&c.cnt->n_next)] = t;
+    if (at_exch(&c.qst[n], (int)c.sr + 1) != (int)c.sr + 1)
+        c.queue_next[append_slot(&c.cnt->n_next)] = n;
+}
+
+GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
+    int4* row = &c.TA[tt];
+    int old = comp(*row, s);
+    if (old < 0) return;
+    int m = old >> 2, ms = old & 3;
+    if (c.fst[m] == (int)c.sr) {
+        ((int*)row)[s] = comp(c.fmap[m], ms);
+    } else {
+        ((int*)&c.TA[m])[ms] = enc(tt, s);
+    }
+}
+
+GCDT_HD void body_flip_fix(const Ctx& c, int k) {
+    int t = c.flipped[k];
+    int n = c.TA[t].y >> 2;
+    resolve_flip_edge(c, t, 0);
+    resolve_flip_edge(c, t, 2);
+    resolve_flip_edge(c, n, 0);
+    resolve_flip_edge(c, n, 1);
+}
+
+// ---------------------------------------------------------------- constraints
+
+// vt[v] = some triangle incident to v.
+GCDT_HD void body_vt(const Ctx& c, int t) {
+    int4 tv = c.TV[t];
+    c.vt[tv.x] = t; c.vt[tv.y] = t; c.vt[tv.z] = t;
+}
+
+// Map segment endpoints to sorted ids; reject malformed segments.
+GCDT_HD void body_seg_init(const Ctx& c, int k) {
+    int2 ab = c.in_cons[k];
+    if (ab.x < 0 || ab.y < 0 || ab.x >= c.n || ab.y >= c.n || ab.x == ab.y) {
+        fail(c, ST_BAD_INPUT);
+        c.seg[k] = make_int4(0, 0, 0, 0);
+    } else {
+        c.seg[k] = make_int4(c.rank[ab.x], c.rank[ab.y], -1, 0);
+    }
+    c.pend[k] = k;
+}
+
+GCDT_HD long long dot3(int2 a, int2 u, int2 b) {  // (u-a).(b-a)
+    return (long long)(u.x - a.x) * (b.x - a.x) + (long long)(u.y - a.y) * (b.y - a.y);
+}
+
+GCDT_HD void mark_edge(const Ctx& c, int t, int s) {
+    at_or(&c.TV[t].w, 1 << s);
+    int en = comp(c.TA[t], s);
+    if (en >= 0) at_or(&c.TV[en >> 2].w, 1 << (en & 3));
+}
+
+// Walk from the current start vertex a of a pending segment towards b.
+// Existing edges along ab (through collinear vertices) are flagged and
+// skipped; the first sub-segment (a, stop) that crosses triangles is
+// recorded: pinfo = (4*t+i of the first crossed edge, triangles crossed).
+// A crossed constraint edge means the input constraints cross.
+GCDT_HD void body_cwalk(const Ctx& c, int k) {
+    int sk = c.pend[k];
+    int4 sg = c.seg[sk];
+    int a = sg.x, b = sg.y;
+    int2 pb = c.P[b];
+    for (int guard = 0; guard <= c.n + 4; ++guard) {
+        if (a == b) {
+            c.seg[sk].x = a;
+            c.pinfo[k] = make_int4(-1, 0, 0, 0);
+            return;
+        }
+        int2 pa = c.P[a];
+        int t0 = c.vt[a], t = t0;
+        int found = -1, fslot = 0, via = -1, et = -1, es = 0;
+        for (int g2 = 0; g2 < (1 << 16); ++g2) {
+            int4 tv = c.TV[t];
+            int i = slot_of(tv, a), i1 = nx3(i), i2 = nx3(i1);
+            int u = comp(tv, i1), w = comp(tv, i2);
+            if (u == b) { via = b; et = t; es = i2; break; }
+            if (w == b) { via = b; et = t; es = i1; break; }
+            int2 pu = c.P[u], pw = c.P[w];
+            int ou = orient2d(pa, pu, pb), ow = orient2d(pa, pw, pb);
+            if (ou == 0 && dot3(pa, pu, pb) > 0) { via = u; et = t; es = i2; break; }
+            if (ow == 0 && dot3(pa, pw, pb) > 0) { via = w; et = t; es = i1; break; }
+            if (ou > 0 && ow < 0) { found = t; fslot = i; break; }
+            int nb = comp(c.TA[t], i2);
+            if (nb < 0) break;
+            t = nb >> 2;
+            if (t == t0) break;
+        }
+        if (via >= 0) {
+            mark_edge(c, et, es);
+            a = via;
+            continue;
+        }
+        if (found < 0) { fail(c, ST_CONSTRAINT_FAIL); c.pinfo[k] = make_int4(-1, 0, 0, 0); return; }
+        int cur = found, cs = fslot, count = 1, stop = -1;
+        for (int steps = 0; steps <= c.ntri; ++steps) {
+            int4 tv = c.TV[cur];
+            if ((tv.w >> cs) & 1) { fail(c, ST_CONSTRAINT_FAIL); c.pinfo[k] = make_int4(-1, 0, 0, 0); return; }
+            int en = comp(c.TA[cur], cs);
+            if (en < 0) { fail(c, ST_CONSTRAINT_FAIL); c.pinfo[k] = make_int4(-1, 0, 0, 0); return; }
+            int n = en >> 2, j = en & 3;
+            int x = comp(c.TV[n], j);
+            count++;
+            if (x == b) { stop = b; break; }
+            int ox = orient2d(pa, pb, c.P[x]);
+            if (ox == 0) { stop = x; break; }
+            cur = n;
+            cs = ox < 0 ? nx3(nx3(j)) : nx3(j);
+        }
+        if (stop < 0) { fail(c, ST_ITER_LIMIT); c.pinfo[k] = make_int4(-1, 0, 0, 0); return; }
+        c.seg[sk] = make_int4(a, b, stop, 0);
+        c.pinfo[k] = make_int4(enc(found, fslot), count, 0, -1);
+        return;
+    }
+    fail(c, ST_ITER_LIMIT);
+    c.pinfo[k] = make_int4(-1, 0, 0, 0);
+}
+
+// Record the crossed triangles of the pending sub-segment and the triangles
+// around them, and claim all of them for this segment (smallest hash32 of
+// the segment id wins, so chains of adjacent segments progress in parallel).
+// Scratch per entry: [0,kt) crossed chain, [kt, 2kt+2) ring, [2kt+2, 3kt+2) queue.
+GCDT_HD void body_cclaim(const Ctx& c, int k) {
+    int4 pi = c.pinfo[k];
+    if (pi.x < 0) return;
+    int sk = c.pend[k];
+    int4 sg = c.seg[sk];
+    int kt = pi.y;
+    int cap = 3 * kt + 4;
+    int base = at_add(&c.cnt->scratch_top, cap);
+    if (base + cap > c.scratch_cap) { c.pinfo[k].w = -2; return; }
+    int* L = c.scratch + base;
+    int* R = L + kt;
+    unsigned long long key = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)sk));
+    int2 pa = c.P[sg.x], pb = c.P[sg.y];
+    int cur = pi.x >> 2, cs = pi.x & 3;
+    L[0] = cur;
+    for (int m = 1; m < kt; ++m) {
+        int en = comp(c.TA[cur], cs);
+        int n = en >> 2, j = en & 3;
+        L[m] = n;
+        if (m == kt - 1) break;
+        int x = comp(c.TV[n], j);
+        int ox = orient2d(pa, pb, c.P[x]);
+        cur = n;
+        cs = ox < 0 ? nx3(nx3(j)) : nx3(j);
+    }
+    int nr = 0;
+    for (int m = 0; m < kt; ++m) {
+        int4 ta = c.TA[L[m]];
+        for (int s = 0; s < 3; ++s) {
+            int en = comp(ta, s);
+            if (en < 0) continue;
+            int nb = en >> 2;
+            if ((m > 0 && nb == L[m - 1]) || (m + 1 < kt && nb == L[m + 1])) continue;
+            if (nr < kt + 2) R[nr++] = nb;
+        }
+    }
+    for (int m = 0; m < kt; ++m) at_max64(&c.claim[L[m]], key);
+    for (int r = 0; r < nr; ++r) at_max64(&c.claim[R[r]], key);
+    c.pinfo[k] = make_int4(pi.x, kt, base, nr);
+}
+
+// Flip the edge opposite slot i of t and update every neighbour in place
+// (the caller owns t, its partner and their neighbours).
+GCDT_HD int flip_local(const Ctx& c, int t, int i) {
+    int4 tv = c.TV[t], ta = c.TA[t];
+    int en = comp(ta, i);
+    int n = en >> 2, j = en & 3;
+    int4 nv = c.TV[n], na = c.TA[n];
+    int i1 = nx3(i), i2 = nx3(i1), j1 = nx3(j), j2 = nx3(j1);
+    int A = comp(tv, i), B = comp(tv, i1), C = comp(tv, i2), D = comp(nv, j);
+    int ft = tv.w, fn = nv.w;
+    int oBD = comp(na, j1), oAB = comp(ta, i2), oDC = comp(na, j2), oCA = comp(ta, i1);
+    c.TV[t] = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
+    c.TA[t] = make_int4(oBD, enc(n, 2), oAB, 0);
+    c.TV[n] = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
+    c.TA[n] = make_int4(oDC, oCA, enc(t, 1), 0);
+    if (oBD >= 0) ((int*)&c.TA[oBD >> 2])[oBD & 3] = enc(t, 0);
+    if (oAB >= 0) ((int*)&c.TA[oAB >> 2])[oAB & 3] = enc(t, 2);
+    if (oDC >= 0) ((int*)&c.TA[oDC >> 2])[oDC & 3] = enc(n, 0);
+    if (oCA >= 0) ((int*)&c.TA[oCA >> 2])[oCA & 3] = enc(n, 1);
+    c.vt[A] = t; c.vt[B] = t; c.vt[D] = t; c.vt[C] = n;
+    return n;
+}
+
+GCDT_HD void push_lawson(const Ctx& c, int t) {
+    if (at_exch(&c.qst[t], (int)c.lawson_sr) != (int)c.lawson_sr)
+        c.lq[at_add(&c.cnt->n_lawson, 1)] = t;
+}
+
+// Owners of all their triangles recover the sub-segment (a, stop) by
+// Sloan's method: flip crossing edges whose quadrilateral is strictly
+// convex until none crosses.  Others retry next round.
+GCDT_HD void body_cproc(const Ctx& c, int k) {
+    int4 pi = c.pinfo[k];
+    int sk = c.pend[k];
+    if (pi.x < 0) return;                              // finished in the walk
+    if (pi.w < 0) { c.pend_next[append_slot(&c.cnt->n_next)] = sk; return; }
+    int kt = pi.y;
+    int* L = c.scratch + pi.z;
+    int* R = L + kt;
+    int* Q = R + kt + 2;
+    unsigned long long key = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)sk));
+    bool own = true;
+    for (int m = 0; m < kt && own; ++m) own = c.claim[L[m]] == key;
+    for (int r = 0; r < pi.w && own; ++r) own = c.claim[R[r]] == key;
+    if (!own) { c.pend_next[append_slot(&c.cnt->n_next)] = sk; return; }
+    int4 sg = c.seg[sk];
+    int a = sg.x, b = sg.y, stop = sg.z;
+    int2 pa = c.P[a], pb = c.P[b];
+    // crossing edges between consecutive chain triangles
+    int qn = 0;
+    for (int m = 0; m + 1 < kt; ++m) {
+        int4 ta = c.TA[L[m]];
+        int s = (ta.x >> 2) == L[m + 1] ? 0 : ((ta.y >> 2) == L[m + 1] ? 1 : 2);
+        Q[qn++] = enc(L[m], s);
+    }
+    int head = 0, size = qn;
+    long long guard = 0, limit = 64LL * (kt + 4) * (kt + 4);
+    while (size > 0) {
+        if (++guard > limit) { fail(c, ST_ITER_LIMIT); return; }
+        int e = Q[head]; head = head + 1 == kt ? 0 : head + 1; size--;
+        int t = e >> 2, i = e & 3;
+        int4 tv = c.TV[t];
+        int en = comp(c.TA[t], i);
+        int n = en >> 2, j = en & 3;
+        int A = comp(tv, i), B = comp(tv, nx3(i)), C = comp(tv, nx3(nx3(i)));
+        int D = comp(c.TV[n], j);
+        int2 PA = c.P[A], PD = c.P[D];
+        int s1 = orient2d(PA, PD, c.P[B]), s2 = orient2d(PA, PD, c.P[C]);
+        int tail = head + size; if (tail >= kt) tail -= kt;
+        if (!((s1 > 0 && s2 < 0) || (s1 < 0 && s2 > 0))) { Q[tail] = e; size++; continue; }
+        int i1 = nx3(i), i2 = nx3(i1), j1 = nx3(j), j2 = nx3(j1);
+        flip_local(c, t, i);
+        for (int r = 0, pos = head; r < size; ++r, pos = pos + 1 == kt ? 0 : pos + 1) {
+            int q = Q[pos];
+            if (q == enc(t, i1)) Q[pos] = enc(n, 1);
+            else if (q == enc(t, i2)) Q[pos] = enc(t, 2);
+            else if (q == enc(n, j1)) Q[pos] = enc(t, 0);
+            else if (q == enc(n, j2)) Q[pos] = enc(n, 0);
+        }
+        int oA = orient2d(pa, pb, PA), oD = orient2d(pa, pb, PD);
+        if ((oA > 0 && oD < 0) || (oA < 0 && oD > 0)) { Q[tail] = enc(t, 1); size++; }
+    }
+    // flag the recovered edge (a, stop) on both sides
+    for (int m = 0; m < kt; ++m) {
+        int4 tv = c.TV[L[m]];
+        bool ha = tv.x == a || tv.y == a || tv.z == a;
+        bool hs = tv.x == stop || tv.y == stop || tv.z == stop;
+        if (ha && hs) {
+            int s3 = 3 - slot_of(tv, a) - slot_of(tv, stop);
+            mark_edge(c, L[m], s3);
+            break;
+        }
+    }
+    for (int m = 0; m < kt; ++m) push_lawson(c, L[m]);
+    c.seg[sk].x = stop;
+    if (stop != b) c.pend_next[append_slot(&c.cnt->n_next)] = sk;
+}
+
+// ---------------------------------------------------------------- output
+
+GCDT_HD void body_output(const Ctx& c, int t) {
+    int4 tv = c.TV[t], ta = c.TA[t];
+    c.out_tris[3 * t + 0] = c.perm[tv.x];
+    c.out_tris[3 * t + 1] = c.perm[tv.y];
+    c.out_tris[3 * t + 2] = c.perm[tv.z];
+    c.out_adj[3 * t + 0] = ta.x < 0 ? -1 : ta.x >> 2;
+    c.out_adj[3 * t + 1] = ta.y < 0 ? -1 : ta.y >> 2;
+    c.out_adj[3 * t + 2] = ta.z < 0 ? -1 : ta.z >> 2;
+    c.out_cflags[t] = (unsigned char)(tv.w & 7);
+}
+
+}  // namespace gcdt

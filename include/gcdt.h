@@ -1,0 +1,101 @@
+/*
+ * gcdt.h -- C ABI of the B200 constrained Delaunay triangulator.
+ *
+ * One entry point replaces the reference's device pipeline for the path
+ *   integer points + segment index pairs -> triangles + adjacency + constraint flags.
+ * In yingtix/gCDT that path is the driver sequence of kernel.cu:5395-5448:
+ *   getSamplePoints (include/rawMesh.h:6), rawMeshBefore (include/rawMesh.h:4),
+ *   filterTriangles (kernel.cu:5293), delaunaySample (kernel.cu:5038),
+ *   getBitmap (include/boostmap.h:4), rawMeshAfter (include/rawMesh.h:5),
+ *   addConstraints (include/addConstraints.h:5), delaunayNew (kernel.cu:4697).
+ * The same-signature C++ symbols of that surface are declared in
+ * gcdt_reference_surface.h.
+ *
+ * Conventions (kept from the reference):
+ *   - points are int32 (x, y) pairs with 1 <= x, y <= 2^30 - 2, pairwise
+ *     distinct; the four box corners (0,0), (R,0), (R,R), (0,R), R = 2^30 - 1,
+ *     are added as vertices n, n+1, n+2, n+3 (rawMesh.cu:5-35);
+ *   - segments are int32 index pairs into the points, non-crossing;
+ *   - the output has exactly 2n + 2 triangles (hull = the box);
+ *   - triangle k = (tris[3k], tris[3k+1], tris[3k+2]) is counter-clockwise;
+ *     adj[3k+i] is the triangle across the edge opposite tris[3k+i], or -1 on
+ *     the box (rawMesh.cu:269-276); bit i of cflags[k] is set when that edge
+ *     is a constraint edge.
+ * Differences from the reference, by design:
+ *   - vertex ids in the output are the caller's input indices (the reference
+ *     returns a Morton-permuted point array, kernel.cu:2059-2066);
+ *   - a segment passing exactly through an input point is split there and
+ *     recovered as two edges (the reference drops it, addConstraints.cu:962-965);
+ *   - cocircular ties are broken by a fixed symbolic perturbation, so the
+ *     output is unique for every input.
+ * All pointers named d_* are device pointers.  Calls on one context must not
+ * overlap; a call returns when its result is complete on `stream`.
+ */
+#ifndef GCDT_H
+#define GCDT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    GCDT_OK = 0,
+    GCDT_BAD_INPUT = 1,        /* range, duplicates, bad segment index */
+    GCDT_OOM = 2,              /* problem larger than the context was created for */
+    GCDT_ITER_LIMIT = 3,       /* a bounded device loop ran out of iterations */
+    GCDT_CONSTRAINT_FAIL = 4,  /* segments cross each other */
+    GCDT_CUDA_ERROR = 5,
+    GCDT_INTERNAL = 6
+} gcdt_status;
+
+typedef struct gcdt_context gcdt_context;
+
+typedef struct {
+    int64_t n_points;
+    int64_t n_segments;
+    int64_t n_triangles;
+    int64_t insertion_rounds;
+    int64_t flip_subrounds;
+    int64_t flips;
+    int64_t constraint_rounds;
+    int64_t host_syncs;
+    int64_t kernel_launches;
+    double device_ms;          /* CUDA-event time of the whole solve */
+} gcdt_stats;
+
+/* Largest point count a context accepts (triangle ids must fit 29 bits). */
+#define GCDT_MAX_POINTS ((int64_t)((1 << 28) - 2))
+
+/* Create a context on `device` whose arena fits max_points / max_segments.
+   Replaces the reference's MemCache pre-pool (MemCache.cpp:60-76). */
+gcdt_status gcdt_create(gcdt_context** ctx, int device, int64_t max_points, int64_t max_segments);
+void gcdt_destroy(gcdt_context* ctx);
+
+/* Device bytes one solve of (n, s) needs. */
+size_t gcdt_workspace_bytes(int64_t n_points, int64_t n_segments);
+
+/* Triangulate.  d_points: 2n int32, d_segments: 2s int32 (may be NULL if
+   s == 0); outputs sized for 2n+2 triangles: d_tris and d_adj 3 int32 each,
+   d_cflags 1 byte each.  *n_tris (host) receives 2n+2 on success. */
+gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_points, int32_t n,
+                             const int32_t* d_segments, int32_t s,
+                             int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                             int32_t* n_tris, void* stream);
+
+gcdt_status gcdt_get_stats(const gcdt_context* ctx, gcdt_stats* out);
+const char* gcdt_status_string(gcdt_status s);
+
+/* Exact predicates on device, for parity tests.  d_quads: 8 int32 per case
+   (a, b, c, d points); d_out: 3 int32 per case = orient2d(a,b,c),
+   inCircle(a,b,c,d) (exact sign, math_base.cuh:267-328) and the perturbed
+   inCircle used by the triangulator. */
+gcdt_status gcdt_eval_predicates(const int32_t* d_quads, int32_t n_cases, int32_t* d_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GCDT_H */
