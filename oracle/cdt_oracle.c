@@ -602,8 +602,9 @@ int oracle_validate(const int32_t *xy, int n, const int32_t *cons, int s,
     qsort(cedges, nce, sizeof(uint64_t), edge_cmp);
     /* every constraint = chain of constrained edges through collinear vertices */
     {
-        uint64_t *used = (uint64_t *)malloc(sizeof(uint64_t) * (nce + 1));
-        size_t nused = 0;
+        size_t ucap = nce + 16, nused = 0;
+        uint64_t *used = (uint64_t *)malloc(sizeof(uint64_t) * ucap);
+        if (!used) FAIL("oom");
         for (int k = 0; k < s; ++k) {
             int a = cons[2 * k], b = cons[2 * k + 1];
             int guard = 0;
@@ -623,6 +624,11 @@ int oracle_validate(const int32_t *xy, int n, const int32_t *cons, int s,
                     free(used); FAIL("constraint %d (%d,%d) missing at vertex %d", k, cons[2 * k], cons[2 * k + 1], a);
                 }
                 if (!edge_in(cedges, nce, a, nxt)) { free(used); FAIL("constraint %d edge (%d,%d) not flagged", k, a, nxt); }
+                if (nused == ucap) {   /* overlapping constraints repeat edges */
+                    uint64_t *nu = (uint64_t *)realloc(used, sizeof(uint64_t) * ucap * 2);
+                    if (!nu) { free(used); FAIL("oom"); }
+                    used = nu; ucap *= 2;
+                }
                 used[nused++] = a < nxt ? ((uint64_t)a << 32) | (uint32_t)nxt : ((uint64_t)nxt << 32) | (uint32_t)a;
                 a = nxt;
             }
