@@ -3,6 +3,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "solver.cuh"
@@ -265,4 +266,87 @@ extern "C" gcdt_status gcdt_eval_predicates(const int32_t* d_quads, int32_t n_ca
     if (cudaGetLastError() != cudaSuccess) return GCDT_CUDA_ERROR;
     if (cudaStreamSynchronize(st) != cudaSuccess) return GCDT_CUDA_ERROR;
     return GCDT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free triangulation.
+//
+// Some callers cannot allocate device memory at call time: a plugin whose host
+// application owns all device memory through its own caching allocator (a
+// cudaMalloc there can fail even with memory free, because the host's pool
+// holds it), or a latency-bound loop that cannot afford cudaMalloc/cudaFree,
+// which may synchronize the whole device.  For them this entry point runs the
+// same solve as gcdt_triangulate with its scratch in one file-scope device
+// array instead of a context arena.  The array is part of this library's
+// module, so every GPU that loads the library holds it until the process
+// exits.
+//
+// Set-up: the first call on each device (made with that device current)
+// looks the array's device address up with cudaGetSymbolAddress; later calls
+// on that device reuse it.  Make that first call before any stream capture
+// begins on the device.
+//
+// Limits and sharing: a problem whose workspace (gcdt_workspace_bytes(n, s))
+// exceeds GCDT_NOALLOC_WORKSPACE_BYTES is rejected with GCDT_OOM before any
+// device work.  All calls on a device share the one array and it keeps the
+// previous call's contents; the solve itself zeroes every array that must
+// start at zero.  Two calls whose work overlaps on the GPU (different
+// streams, or different host threads) race on the array and corrupt each
+// other's results: serialize them.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoAllocBytes = GCDT_NOALLOC_WORKSPACE_BYTES;
+__device__ __align__(256) unsigned char g_noalloc_workspace[kNoAllocBytes];
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+char* g_noalloc_base[kNoAllocMaxDevices] = {};
+}  // namespace
+
+extern "C" gcdt_status gcdt_triangulate_noalloc(const int32_t* d_points, int32_t n,
+                                                const int32_t* d_segments, int32_t s,
+                                                int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                                int32_t* n_tris, void* stream) {
+    if (n < 0 || s < 0 || (n > 0 && !d_points) || (s > 0 && !d_segments) || !d_tris || !d_adj || !d_cflags)
+        return GCDT_BAD_INPUT;
+    Plan plan = make_plan(n, s, sort_temp_bytes(n));
+    if (plan.L.total > kNoAllocBytes) return GCDT_OOM;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        cudaGetLastError();
+        return GCDT_CUDA_ERROR;
+    }
+    char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_base[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_workspace);
+            if (e != cudaSuccess || !p) {
+                cudaGetLastError();
+                return GCDT_CUDA_ERROR;
+            }
+            g_noalloc_base[dev] = static_cast<char*>(p);
+        }
+        base = g_noalloc_base[dev];
+    }
+    Ctx c = bind_ctx(base, plan);
+    c.in_xy = reinterpret_cast<const int2*>(d_points);
+    c.in_cons = reinterpret_cast<const int2*>(d_segments);
+    c.out_tris = d_tris;
+    c.out_adj = d_adj;
+    c.out_cflags = d_cflags;
+    Counters host_counters;   // pageable: counter reads go through cudaMemcpyAsync + sync
+    DeviceBackend bk;
+    bk.st = static_cast<cudaStream_t>(stream);
+    bk.dcnt = c.cnt;
+    bk.hcnt = &host_counters;
+    bk.sort_tmp = base + plan.o_sort_tmp;
+    bk.sort_bytes = plan.sort_temp_bytes;
+    SolveStats st;
+    int bits = run_solve(bk, c, st);
+    bk.note(cudaStreamSynchronize(bk.st));
+    if (bk.err != cudaSuccess) bits |= ST_CUDA;
+    gcdt_status rc = map_status(bits);
+    if (rc == GCDT_OK && n_tris) *n_tris = 2 * n + 2;
+    return rc;
 }

@@ -94,6 +94,27 @@ const char* gcdt_status_string(gcdt_status s);
    inCircle used by the triangulator. */
 gcdt_status gcdt_eval_predicates(const int32_t* d_quads, int32_t n_cases, int32_t* d_out, void* stream);
 
+/* Allocation-free variant of gcdt_triangulate (no counterpart in the
+   reference, whose stages all allocate from its MemCache pool).  For callers
+   that cannot allocate device memory when they call in: plugins whose host
+   application owns the device memory through its own caching allocator, and
+   latency-bound loops that cannot pay for cudaMalloc/cudaFree (which may
+   synchronize the device).  Scratch lives in one static device array of
+   GCDT_NOALLOC_WORKSPACE_BYTES inside this library, held by every GPU that
+   loads it until the process exits.  The first call on a device (with that
+   device current) looks up the array's address; make that call before any
+   stream capture starts.  Problems needing more workspace than the array
+   (gcdt_workspace_bytes(n, s) > GCDT_NOALLOC_WORKSPACE_BYTES, about 100,000
+   points) return GCDT_OOM without touching the device.  Calls share the
+   array: calls that overlap on the GPU race and corrupt each other, so
+   serialize them.  Inputs and outputs are as for gcdt_triangulate; the
+   caller passes the device buffers, and the call allocates nothing. */
+#define GCDT_NOALLOC_WORKSPACE_BYTES ((size_t)32 << 20)
+gcdt_status gcdt_triangulate_noalloc(const int32_t* d_points, int32_t n,
+                                     const int32_t* d_segments, int32_t s,
+                                     int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                     int32_t* n_tris, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
