@@ -22,19 +22,9 @@ constexpr int kBlock = 256;
 GCDT_KERNEL(gcdt_keys, body_keys)
 GCDT_KERNEL(gcdt_gather, body_gather)
 GCDT_KERNEL(gcdt_root, body_root)
-GCDT_KERNEL(gcdt_initloc, body_initloc)
-GCDT_KERNEL(gcdt_reloc_vote, body_reloc_vote)
-GCDT_KERNEL(gcdt_split, body_split)
-GCDT_KERNEL(gcdt_fix, body_fix)
-GCDT_KERNEL(gcdt_flip_check, body_flip_check)
-GCDT_KERNEL(gcdt_flip_do, body_flip_do)
-GCDT_KERNEL(gcdt_flip_fix, body_flip_fix)
-GCDT_KERNEL(gcdt_output, body_output)
-GCDT_KERNEL(gcdt_vt, body_vt)
+GCDT_KERNEL(gcdt_level, body_level)
+GCDT_KERNEL(gcdt_seg_level0, body_seg_level0)
 GCDT_KERNEL(gcdt_seg_init, body_seg_init)
-GCDT_KERNEL(gcdt_cwalk, body_cwalk)
-GCDT_KERNEL(gcdt_cclaim, body_cclaim)
-GCDT_KERNEL(gcdt_cproc, body_cproc)
 
 __global__ void gcdt_predicates(const int2* q, int n, int* out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -43,6 +33,72 @@ __global__ void gcdt_predicates(const int2* q, int n, int* out) {
     out[3 * i] = orient2d(a, b, cc);
     out[3 * i + 1] = incircle(a, b, cc, d);
     out[3 * i + 2] = incircle_sos(a, b, cc, d);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent stage kernel.  One cooperative launch runs every insertion
+// round, flip sub-round and constraint round of a solve; phases are
+// grid-stride loops separated by a grid barrier, so the round structure
+// costs no kernel launches and no host round trips.
+
+constexpr int kPersistBlock = 256;
+
+struct GridExec {
+    Counters* cnt;
+    unsigned nblocks;
+
+    // Sense-free generation barrier.  Every wait is bounded: after ~2^24
+    // polls the block records ST_BARRIER and stops waiting, and once that bit
+    // is set no block waits or works any more, so the kernel always ends.
+    __device__ void barrier() {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            volatile unsigned* vgen = &cnt->bar_gen;
+            volatile int* vst = &cnt->status;
+            if (!(*vst & ST_BARRIER)) {
+                unsigned g = *vgen;
+                __threadfence();
+                unsigned arrived = atomicAdd(&cnt->bar_count, 1u);
+                if (arrived == nblocks - 1) {
+                    atomicExch(&cnt->bar_count, 0u);
+                    __threadfence();
+                    atomicAdd(&cnt->bar_gen, 1u);
+                } else {
+                    unsigned spins = 0;
+                    while (*vgen == g) {
+                        if (++spins > (1u << 24)) { atomicOr(&cnt->status, ST_BARRIER); break; }
+                        if (*vst & ST_BARRIER) break;
+                        __nanosleep(64);
+                    }
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+    }
+    __device__ void phase(int k, const Ctx& c, long long count) {
+        if (!(word(&cnt->status) & ST_BARRIER)) {
+            long long stride = (long long)gridDim.x * blockDim.x;
+            for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+                dispatch(k, c, (int)i);
+        }
+        barrier();
+    }
+    __device__ unsigned long long cursor(unsigned long long* p) { return *(volatile unsigned long long*)p; }
+    __device__ int word(int* p) { return *(volatile int*)p; }
+    __device__ void finish(const Ctx&, long long rounds, long long subrounds, long long crounds, int rc) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            cnt->rounds = rounds;
+            cnt->flip_subrounds = subrounds;
+            cnt->constraint_rounds = crounds;
+            if (rc) atomicOr(&cnt->status, rc);
+        }
+    }
+};
+
+__global__ void __launch_bounds__(kPersistBlock, 2) gcdt_stages(Ctx c) {
+    GridExec ex{c.cnt, gridDim.x};
+    run_stages(ex, c);
 }
 
 constexpr int ST_CUDA = 32;
@@ -66,27 +122,30 @@ struct DeviceBackend {
         case K_KEYS: gcdt_keys<<<grid, kBlock, 0, st>>>(c, nn); break;
         case K_GATHER: gcdt_gather<<<grid, kBlock, 0, st>>>(c, nn); break;
         case K_ROOT: gcdt_root<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_INITLOC: gcdt_initloc<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_RELOC_VOTE: gcdt_reloc_vote<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_SPLIT: gcdt_split<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_FIX: gcdt_fix<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_FLIP_CHECK: gcdt_flip_check<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_FLIP_DO: gcdt_flip_do<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_FLIP_FIX: gcdt_flip_fix<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_OUTPUT: gcdt_output<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_VT: gcdt_vt<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_LEVEL: gcdt_level<<<grid, kBlock, 0, st>>>(c, nn); break;
+        case K_SEG_LEVEL0: gcdt_seg_level0<<<grid, kBlock, 0, st>>>(c, nn); break;
         case K_SEG_INIT: gcdt_seg_init<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_CWALK: gcdt_cwalk<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_CCLAIM: gcdt_cclaim<<<grid, kBlock, 0, st>>>(c, nn); break;
-        case K_CPROC: gcdt_cproc<<<grid, kBlock, 0, st>>>(c, nn); break;
-        default: break;
+        default: note(cudaErrorInvalidValue); return;
         }
         launches++;
         note(cudaGetLastError());
     }
     void fill(void* p, int v, size_t bytes) { note(cudaMemsetAsync(p, v, bytes, st)); }
-    void reset_lists() { note(cudaMemsetAsync(&dcnt->n_next, 0, 3 * sizeof(int), st)); }
-    void set_scratch_top(int) { note(cudaMemsetAsync(&dcnt->scratch_top, 0, sizeof(int), st)); }
+    // All rounds run in one cooperative launch sized to the co-resident
+    // block count, so every block is resident and the grid barrier is safe.
+    void stages(const Ctx& c) {
+        if (err != cudaSuccess) return;
+        int dev = 0, sms = 0, per_sm = 0;
+        note(cudaGetDevice(&dev));
+        note(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        note(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gcdt_stages, kPersistBlock, 0));
+        if (err != cudaSuccess || sms <= 0 || per_sm <= 0) { note(cudaErrorLaunchOutOfResources); return; }
+        Ctx cc = c;
+        void* args[] = {&cc};
+        note(cudaLaunchCooperativeKernel((const void*)gcdt_stages, dim3(sms * per_sm), dim3(kPersistBlock),
+                                         args, 0, st));
+        launches++;
+    }
     void read(Counters* h) {
         note(cudaMemcpyAsync(hcnt, dcnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
         note(cudaStreamSynchronize(st));
@@ -119,7 +178,7 @@ inline gcdt_status map_status(int bits) {
     if (bits & ST_CONSTRAINT_FAIL) return GCDT_CONSTRAINT_FAIL;
     if (bits & ST_ITER_LIMIT) return GCDT_ITER_LIMIT;
     if (bits & ST_OOM) return GCDT_OOM;
-    return GCDT_INTERNAL;
+    return GCDT_INTERNAL;   // ST_INTERNAL, ST_BARRIER
 }
 
 }  // namespace gcdt

@@ -28,7 +28,7 @@ struct Plan {
     size_t o_keys, o_keys_alt, o_vals, o_vals_alt, o_sort_tmp;
     size_t o_P, o_perm, o_rank, o_TV, o_TA, o_loc, o_pedge, o_actA, o_actB, o_vote, o_ins, o_modR, o_win;
     size_t o_claim, o_cand, o_fmap, o_fst, o_qst, o_qA, o_qB, o_flipped;
-    size_t o_seg, o_pendA, o_pendB, o_pinfo, o_scratch, o_vt, o_cnt;
+    size_t o_seg, o_pendA, o_pendB, o_pinfo, o_scratch, o_vt, o_lvl, o_cnt;
 };
 
 inline Plan make_plan(int64_t n, int64_t s, size_t sort_temp_bytes) {
@@ -71,6 +71,7 @@ inline Plan make_plan(int64_t n, int64_t s, size_t sort_temp_bytes) {
     p.o_pinfo = L.take(16 * ss);
     p.o_scratch = L.take(4 * p.scratch_cap);
     p.o_vt = L.take(4 * (nn + 4));
+    p.o_lvl = L.take(nn);
     return p;
 }
 

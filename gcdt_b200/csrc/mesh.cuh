@@ -42,21 +42,28 @@ enum StatusBits : int {
     ST_ITER_LIMIT = 4,
     ST_CONSTRAINT_FAIL = 8,
     ST_INTERNAL = 16,
+    ST_BARRIER = 64,     // a grid barrier wait ran out of iterations
 };
 
-// Device-resident counters; one 128-byte line.
+// Device-resident counters.  Every list has a monotone 64-bit append
+// cursor: a phase appends at [base, cursor) where base is the cursor value
+// when the phase began, so no counter is ever reset between phases.
 struct Counters {
-    int status;          // OR of StatusBits
-    int n_next;          // size of the list being appended to
-    int n_win;           // points inserted this round
-    int n_flip;          // flips performed this sub-round
-    int scratch_top;     // bump allocator of the constraint scratch
-    int n_done;          // segments finished this round
-    int n_lawson;        // triangles queued for the constrained flip pass
-    int pad1;
-    unsigned long long flips_total;
-    unsigned long long walk_steps;
-    unsigned long long pad2[4];
+    int status;                  // OR of StatusBits (host launches, final result)
+    int err[2];                  // errors of the persistent phases, by phase parity
+    int pad0;
+    unsigned long long cur_act0; // lists built by activation
+    unsigned long long cur_act;  // active point lists
+    unsigned long long cur_win;  // inserted points of a round
+    unsigned long long cur_q;    // flip queues
+    unsigned long long cur_flip; // flips of a sub-round
+    unsigned long long cur_pend; // pending segment lists
+    unsigned long long cur_law;  // constrained flip pass queue
+    unsigned long long cur_scr;  // constraint scratch
+    unsigned int bar_count;      // grid barrier
+    unsigned int bar_gen;
+    long long rounds, flip_subrounds, constraint_rounds;
+    long long pad1[3];
 };
 
 struct Ctx {
@@ -65,6 +72,7 @@ struct Ctx {
     int ntri;       // 2n + 2
     unsigned round; // insertion round / epoch stamp
     unsigned sr;    // flip sub-round stamp (monotone over the whole solve)
+    int eslot;      // error word of the running phase (phase parity)
     unsigned lawson_sr;  // queue stamp of the constrained flip pass
     int list_n;     // length of the list a launch iterates over
 
@@ -109,6 +117,14 @@ struct Ctx {
     int scratch_cap;
     int* vt;            // vertex -> incident triangle
     int* lq;            // triangles queued for the constrained flip pass
+
+    // append bases of the lists the current phase writes (see Counters)
+    unsigned long long base_act, base_win, base_q, base_flip, base_pend, base_law, base_scr;
+
+    unsigned char* lvl; // insertion level of each sorted point
+    int level;          // level being activated / the live levels are < level
+    int nlevels;
+    int stride[4];      // level l holds the points i with i % stride[l] == 0 not in a lower level
 
     int* out_tris;
     int* out_adj;
@@ -170,20 +186,24 @@ GCDT_HD int at_or(int* p, int v) {
     int o = *p; *p = o | v; return o;
 #endif
 }
-GCDT_HD void fail(const Ctx& c, int bits) { at_or(&c.cnt->status, bits); }
+// Errors go to the word of the running phase's parity: the driver reads
+// that word after the phase's barrier, while the next phase writes the
+// other one, so every thread sees the same error state.
+GCDT_HD void fail(const Ctx& c, int bits) { at_or(&c.cnt->err[c.eslot], bits); }
 
-// Append one element to a list whose length lives at *ctr.  On the GPU the
-// threads of a warp that append together take one atomic between them.
-GCDT_HD int append_slot(int* ctr) {
+// Append one element to a list with cursor *cur and phase base `base`;
+// returns the element's index in the list.  On the GPU the threads of a warp
+// that append together take one atomic between them.
+GCDT_HD int append_slot(unsigned long long* cur, unsigned long long base) {
 #if defined(__CUDA_ARCH__)
     namespace cg = cooperative_groups;
     cg::coalesced_group g = cg::coalesced_threads();
-    int base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(ctr, (int)g.size());
-    base = g.shfl(base, 0);
-    return base + (int)g.thread_rank();
+    unsigned long long b = 0;
+    if (g.thread_rank() == 0) b = atomicAdd(cur, (unsigned long long)g.size());
+    b = g.shfl(b, 0);
+    return (int)(b - base) + (int)g.thread_rank();
 #else
-    int o = *ctr; *ctr = o + 1; return o;
+    unsigned long long o = *cur; *cur = o + 1; return (int)(o - base);
 #endif
 }
 
@@ -220,8 +240,6 @@ GCDT_HD void body_gather(const Ctx& c, int i) {
         c.perm[i] = j;
         c.rank[j] = i;
         if (i > 0 && c.keys[i] == c.keys[i - 1]) fail(c, ST_BAD_INPUT);
-        c.loc[i] = 0;
-        c.act[i] = i;
     } else if (i < c.n + 4) {
         int k = i - c.n;
         int2 corner;
@@ -241,11 +259,119 @@ GCDT_HD void body_root(const Ctx& c, int) {
     c.TA[1] = make_int4(-1, enc(0, 0), -1, 0);
 }
 
-// Root triangle of each point: orient against the diagonal (R,0)-(0,R)
-// (rawMesh.cu:37-57); a point on the diagonal is in the closed triangle 0.
-GCDT_HD void body_initloc(const Ctx& c, int i) {
-    int2 rd = make_int2(kBoxMax, 0), lt = make_int2(0, kBoxMax);
-    c.loc[i] = orient2d(rd, lt, c.P[i]) >= 0 ? 0 : 1;
+// Level of each sorted point: a Morton-stratified sample first (every
+// stride[0]-th point), then denser samples, then the rest (a biased
+// randomized insertion order over the spatial sort).
+GCDT_HD void body_level(const Ctx& c, int i) {
+    int l = c.nlevels - 1;
+    for (int k = 0; k + 1 < c.nlevels; ++k)
+        if (i % c.stride[k] == 0) { l = k; break; }
+    c.lvl[i] = (unsigned char)l;
+}
+
+GCDT_HD void body_seg_level0(const Ctx& c, int k) {
+    int4 sg = c.seg[k];
+    if (sg.z == -1) { c.lvl[sg.x] = 0; c.lvl[sg.y] = 0; }
+}
+
+GCDT_HD long long dot3(int2 a, int2 u, int2 b) {  // (u-a).(b-a)
+    return (long long)(u.x - a.x) * (b.x - a.x) + (long long)(u.y - a.y) * (b.y - a.y);
+}
+
+// Straight-line walk from vertex a (t: a triangle incident to a) to the
+// triangle whose closed interior holds p (p is not a vertex).  Each step
+// advances along the segment a->p, so the walk ends in any triangulation,
+// constrained or not; a line through a vertex restarts from that vertex.
+GCDT_HD int locate_from_vertex(const Ctx& c, int a, int t, int2 p) {
+    for (int restart = 0; restart < 4096; ++restart) {
+        int2 pa = c.P[a];
+        int t0 = t, found = -1, fslot = 0, u = -1, w = -1;
+        for (int g = 0; g < 4096; ++g) {
+            int4 tv = c.TV[t];
+            int i = slot_of(tv, a), i1 = nx3(i), i2 = nx3(i1);
+            u = comp(tv, i1); w = comp(tv, i2);
+            int2 pu = c.P[u], pw = c.P[w];
+            int ou = orient2d(pa, pu, p), ow = orient2d(pa, pw, p);
+            if (ou == 0 && dot3(pa, pu, p) > 0) {
+                if (dot3(pa, p, pu) > dot3(pa, p, p)) return t;   // p inside edge (a,u)
+                found = -2; a = u; break;                          // continue from u
+            }
+            if (ow == 0 && dot3(pa, pw, p) > 0) {
+                if (dot3(pa, p, pw) > dot3(pa, p, p)) return t;
+                found = -2; a = w; break;
+            }
+            if (ou > 0 && ow < 0) {
+                if (orient2d(pu, pw, p) >= 0) return t;
+                found = t; fslot = i; break;
+            }
+            int nb = comp(c.TA[t], i2);
+            if (nb < 0) return -1;
+            t = nb >> 2;
+            if (t == t0) return -1;
+        }
+        if (found == -2) continue;          // t contains the new a
+        if (found < 0) return -1;
+        int cur = found, cs = fslot;
+        int next_a = -1;
+        for (int steps = 0; steps < (1 << 22); ++steps) {
+            int en = comp(c.TA[cur], cs);
+            if (en < 0) return -1;
+            int n = en >> 2, j = en & 3;
+            int x = comp(c.TV[n], j);
+            int2 px = c.P[x];
+            // n = (x, w, u): p is inside iff it is left of (u,x) and (x,w)
+            if (orient2d(c.P[u], px, p) >= 0 && orient2d(px, c.P[w], p) >= 0) return n;
+            int ox = orient2d(pa, p, px);
+            if (ox == 0) { next_a = x; t = n; break; }
+            cur = n;
+            if (ox < 0) { u = x; cs = nx3(nx3(j)); } else { w = x; cs = nx3(j); }
+        }
+        if (next_a < 0) return -1;
+        a = next_a;
+    }
+    return -1;
+}
+
+// Put the points of level c.level into the active list with their
+// triangle: the root triangles for level 0 (orient against the diagonal
+// (R,0)-(0,R), rawMesh.cu:37-57), otherwise a straight-line walk from the
+// Morton-preceding point of the previous level, which is already a vertex.
+GCDT_HD void body_activate(const Ctx& c, int i) {
+    if (c.lvl[i] != c.level) return;
+    int t;
+    if (c.level == 0) {
+        int2 rd = make_int2(kBoxMax, 0), lt = make_int2(0, kBoxMax);
+        t = orient2d(rd, lt, c.P[i]) >= 0 ? 0 : 1;
+    } else {
+        int sv = i - i % c.stride[c.level - 1];
+        t = locate_from_vertex(c, sv, c.vt[sv], c.P[i]);
+        if (t < 0) { fail(c, ST_ITER_LIMIT); return; }
+    }
+    c.loc[i] = t;
+    c.act_next[append_slot(&c.cnt->cur_act0, c.base_act)] = i;
+}
+
+GCDT_HD int at_min(int* p, int v) {
+#if defined(__CUDA_ARCH__)
+    return atomicMin(p, v);
+#else
+    int o = *p; if (v < o) *p = v; return o;
+#endif
+}
+
+GCDT_HD void body_vt_reset(const Ctx& c, int v) { c.vt[v] = 0x7fffffff; }
+
+// vt[v] = the smallest live triangle incident to v (deterministic, so walks
+// that start from vt give the same result on every run).  Live triangles:
+// the root slots 0 and 1, and the two slots of each inserted point (points
+// of level < c.level); k < n + 2.
+GCDT_HD void body_vt_live(const Ctx& c, int k) {
+    if (k >= 2 && c.lvl[k - 2] >= c.level) return;
+    int t0 = k < 2 ? k : 2 * k - 2, nt = k < 2 ? 1 : 2;
+    for (int t = t0; t < t0 + nt; ++t) {
+        int4 tv = c.TV[t];
+        at_min(&c.vt[tv.x], t); at_min(&c.vt[tv.y], t); at_min(&c.vt[tv.z], t);
+    }
 }
 
 // ---------------------------------------------------------------- insertion
@@ -283,12 +409,13 @@ GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
     int2 p = c.P[q];
     if (c.modR[t] == (int)c.round - 1) {
         int steps = 0;
-        int nt = walk(c, t, p, 1 << 20, &steps);
+        int nt = walk(c, t, p, 256, &steps);
+        if (nt < 0) nt = locate_from_vertex(c, c.TV[t].x, t, p);
         if (nt < 0) { fail(c, ST_ITER_LIMIT); return; }
         t = nt;
         c.loc[q] = t;
     }
-    c.act_next[append_slot(&c.cnt->n_next)] = q;
+    c.act_next[append_slot(&c.cnt->cur_act, c.base_act)] = q;
     int4 tv = c.TV[t];
     int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
     int o0 = orient2d(b, cc, p), o1 = orient2d(cc, a, p), o2 = orient2d(a, b, p);
@@ -365,7 +492,7 @@ GCDT_HD void body_split(const Ctx& c, int k) {
         c.modR[n] = (int)c.round;
     }
     c.loc[q] = -1;
-    c.winners[append_slot(&c.cnt->n_win)] = make_int2(q, t);
+    c.winners[append_slot(&c.cnt->cur_win, c.base_win)] = make_int2(q, t);
 }
 
 // Child of triangle m (split this round) that now holds m's old edge `ms`.
@@ -379,7 +506,7 @@ GCDT_HD int split_child(int2 im, int m, int ms) {
 
 GCDT_HD void push_queue(const Ctx& c, int t) {
     if (at_exch(&c.qst[t], (int)c.sr) != (int)c.sr)
-        c.queue_next[append_slot(&c.cnt->n_next)] = t;
+        c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = t;
 }
 
 GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
@@ -460,7 +587,7 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     if (c.claim[t] != ck || c.claim[n] != ck) {
         // re-check next sub-round; stamp sr+1 is the next queue's stamp
         if (at_exch(&c.qst[t], (int)c.sr + 1) != (int)c.sr + 1)
-            c.queue_next[append_slot(&c.cnt->n_next)] = t;
+            c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = t;
         return;
     }
     int4 tv = c.TV[t], ta = c.TA[t], nv = c.TV[n], na = c.TA[n];
@@ -480,11 +607,11 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     c.fst[n] = (int)c.sr;
     c.modR[t] = (int)c.round;
     c.modR[n] = (int)c.round;
-    c.flipped[append_slot(&c.cnt->n_flip)] = t;
+    c.flipped[append_slot(&c.cnt->cur_flip, c.base_flip)] = t;
     if (at_exch(&c.qst[t], (int)c.sr + 1) != (int)c.sr + 1)
-        c.queue_next[append_slot(&c.cnt->n_next)] = t;
+        c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = t;
     if (at_exch(&c.qst[n], (int)c.sr + 1) != (int)c.sr + 1)
-        c.queue_next[append_slot(&c.cnt->n_next)] = n;
+        c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = n;
 }
 
 GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
@@ -510,26 +637,16 @@ GCDT_HD void body_flip_fix(const Ctx& c, int k) {
 
 // ---------------------------------------------------------------- constraints
 
-// vt[v] = some triangle incident to v.
-GCDT_HD void body_vt(const Ctx& c, int t) {
-    int4 tv = c.TV[t];
-    c.vt[tv.x] = t; c.vt[tv.y] = t; c.vt[tv.z] = t;
-}
-
 // Map segment endpoints to sorted ids; reject malformed segments.
 GCDT_HD void body_seg_init(const Ctx& c, int k) {
     int2 ab = c.in_cons[k];
     if (ab.x < 0 || ab.y < 0 || ab.x >= c.n || ab.y >= c.n || ab.x == ab.y) {
         fail(c, ST_BAD_INPUT);
-        c.seg[k] = make_int4(0, 0, 0, 0);
+        c.seg[k] = make_int4(0, 0, 0, 0);   // .z != -1: not a valid segment
     } else {
         c.seg[k] = make_int4(c.rank[ab.x], c.rank[ab.y], -1, 0);
     }
     c.pend[k] = k;
-}
-
-GCDT_HD long long dot3(int2 a, int2 u, int2 b) {  // (u-a).(b-a)
-    return (long long)(u.x - a.x) * (b.x - a.x) + (long long)(u.y - a.y) * (b.y - a.y);
 }
 
 GCDT_HD void mark_edge(const Ctx& c, int t, int s) {
@@ -614,8 +731,9 @@ GCDT_HD void body_cclaim(const Ctx& c, int k) {
     int4 sg = c.seg[sk];
     int kt = pi.y;
     int cap = 3 * kt + 4;
-    int base = at_add(&c.cnt->scratch_top, cap);
-    if (base + cap > c.scratch_cap) { c.pinfo[k].w = -2; return; }
+    unsigned long long b0 = at_add64(&c.cnt->cur_scr, (unsigned long long)cap) - c.base_scr;
+    if (b0 + cap > (unsigned long long)c.scratch_cap) { c.pinfo[k].w = -2; return; }
+    int base = (int)b0;
     int* L = c.scratch + base;
     int* R = L + kt;
     unsigned long long key = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)sk));
@@ -673,7 +791,7 @@ GCDT_HD int flip_local(const Ctx& c, int t, int i) {
 
 GCDT_HD void push_lawson(const Ctx& c, int t) {
     if (at_exch(&c.qst[t], (int)c.lawson_sr) != (int)c.lawson_sr)
-        c.lq[at_add(&c.cnt->n_lawson, 1)] = t;
+        c.lq[append_slot(&c.cnt->cur_law, c.base_law)] = t;
 }
 
 // Owners of all their triangles recover the sub-segment (a, stop) by
@@ -683,7 +801,7 @@ GCDT_HD void body_cproc(const Ctx& c, int k) {
     int4 pi = c.pinfo[k];
     int sk = c.pend[k];
     if (pi.x < 0) return;                              // finished in the walk
-    if (pi.w < 0) { c.pend_next[append_slot(&c.cnt->n_next)] = sk; return; }
+    if (pi.w < 0) { c.pend_next[append_slot(&c.cnt->cur_pend, c.base_pend)] = sk; return; }
     int kt = pi.y;
     int* L = c.scratch + pi.z;
     int* R = L + kt;
@@ -692,7 +810,7 @@ GCDT_HD void body_cproc(const Ctx& c, int k) {
     bool own = true;
     for (int m = 0; m < kt && own; ++m) own = c.claim[L[m]] == key;
     for (int r = 0; r < pi.w && own; ++r) own = c.claim[R[r]] == key;
-    if (!own) { c.pend_next[append_slot(&c.cnt->n_next)] = sk; return; }
+    if (!own) { c.pend_next[append_slot(&c.cnt->cur_pend, c.base_pend)] = sk; return; }
     int4 sg = c.seg[sk];
     int a = sg.x, b = sg.y, stop = sg.z;
     int2 pa = c.P[a], pb = c.P[b];
@@ -743,7 +861,7 @@ GCDT_HD void body_cproc(const Ctx& c, int k) {
     }
     for (int m = 0; m < kt; ++m) push_lawson(c, L[m]);
     c.seg[sk].x = stop;
-    if (stop != b) c.pend_next[append_slot(&c.cnt->n_next)] = sk;
+    if (stop != b) c.pend_next[append_slot(&c.cnt->cur_pend, c.base_pend)] = sk;
 }
 
 // ---------------------------------------------------------------- output

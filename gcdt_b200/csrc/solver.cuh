@@ -19,9 +19,10 @@
 namespace gcdt {
 
 enum Kern : int {
-    K_KEYS, K_GATHER, K_ROOT, K_INITLOC, K_RELOC_VOTE, K_SPLIT, K_FIX,
+    K_KEYS, K_GATHER, K_ROOT, K_LEVEL, K_SEG_LEVEL0, K_ACTIVATE, K_VT_RESET, K_VT_LIVE,
+    K_RELOC_VOTE, K_SPLIT, K_FIX,
     K_FLIP_CHECK, K_FLIP_DO, K_FLIP_FIX, K_OUTPUT,
-    K_VT, K_SEG_INIT, K_CWALK, K_CCLAIM, K_CPROC,
+    K_SEG_INIT, K_CWALK, K_CCLAIM, K_CPROC,
     K_COUNT
 };
 
@@ -69,7 +70,12 @@ inline Ctx bind_ctx(char* base, const Plan& p) {
     c.scratch = (int*)(base + p.o_scratch);
     c.scratch_cap = (int)p.scratch_cap;
     c.vt = (int*)(base + p.o_vt);
+    c.lvl = (unsigned char*)(base + p.o_lvl);
     c.cnt = (Counters*)(base + p.o_cnt);
+    // two levels: every 64th point of the Morton order plus all segment
+    // endpoints, then the rest
+    c.nlevels = 2;
+    c.stride[0] = 64; c.stride[1] = 1; c.stride[2] = 1; c.stride[3] = 1;
     return c;
 }
 
@@ -79,7 +85,11 @@ GCDT_HD void dispatch(int k, const Ctx& c, int i) {
     case K_KEYS: body_keys(c, i); break;
     case K_GATHER: body_gather(c, i); break;
     case K_ROOT: body_root(c, i); break;
-    case K_INITLOC: body_initloc(c, i); break;
+    case K_LEVEL: body_level(c, i); break;
+    case K_SEG_LEVEL0: body_seg_level0(c, i); break;
+    case K_ACTIVATE: body_activate(c, i); break;
+    case K_VT_RESET: body_vt_reset(c, i); break;
+    case K_VT_LIVE: body_vt_live(c, i); break;
     case K_RELOC_VOTE: body_reloc_vote(c, i); break;
     case K_SPLIT: body_split(c, i); break;
     case K_FIX: body_fix(c, i); break;
@@ -87,7 +97,6 @@ GCDT_HD void dispatch(int k, const Ctx& c, int i) {
     case K_FLIP_DO: body_flip_do(c, i); break;
     case K_FLIP_FIX: body_flip_fix(c, i); break;
     case K_OUTPUT: body_output(c, i); break;
-    case K_VT: body_vt(c, i); break;
     case K_SEG_INIT: body_seg_init(c, i); break;
     case K_CWALK: body_cwalk(c, i); break;
     case K_CCLAIM: body_cclaim(c, i); break;
@@ -100,33 +109,168 @@ constexpr long long kMaxSubrounds = 1 << 20;
 constexpr long long kMaxRounds = 1 << 16;
 constexpr unsigned kMaxConstraintRounds = 1 << 14;
 
-// Flip sub-rounds until the queue is empty.  `qa` holds nq entries stamped
-// `sr`; returns the next free stamp through `sr`.
-template <class BK>
-int flip_until_delaunay(BK& bk, Ctx& c, int*& qa, int*& qb, int nq, unsigned& sr, SolveStats& st) {
-    Counters h;
+// The stage driver runs the same control flow on every GPU thread of the
+// persistent kernel (EX = grid executor: a phase is a grid-stride loop
+// followed by a grid barrier) and on the host for the CPU emulation
+// (EX = sequential executor).  Every value the driver branches on is read
+// right after a barrier and cannot change before the next barrier, so all
+// threads take the same branches:
+//   - a list cursor is read right after the phase that appended to it, and
+//     the phase after that never appends to the same cursor;
+//   - errors of phase k go to err[k & 1], read after phase k's barrier
+//     while phase k+1 writes err[(k+1) & 1].
+//
+// EX provides: phase(kernel, ctx, count), cursor(u64*) -> u64,
+// word(int*) -> int, finish(...).
+
+struct Driver {
+    int* actA; int* actB; int* qa; int* qb;
+    unsigned round, sr;
+    long long rounds, subrounds, crounds;
+    unsigned long long e_act0, e_act, e_win, e_q, e_flip, e_pend, e_law, e_scr;
+    int nphase;
+    int errs;
+};
+
+template <class EX>
+GCDT_HD void run_phase(EX& ex, Ctx& c, Driver& D, int k, long long count) {
+    c.eslot = D.nphase & 1;
+    ex.phase(k, c, count);
+    D.errs |= ex.word(&c.cnt->err[c.eslot]);
+    D.nphase++;
+}
+
+// Flip sub-rounds until the queue `D.qa` (nq entries, stamped D.sr) is empty.
+template <class EX>
+GCDT_HD int flip_until_delaunay(EX& ex, Ctx& c, Driver& D, long long nq) {
     long long guard = 0;
     while (nq > 0) {
         if (++guard > kMaxSubrounds) return ST_ITER_LIMIT;
-        c.queue = qa; c.queue_next = qb; c.sr = sr;
-        bk.reset_lists();
-        bk.launch(K_FLIP_CHECK, c, nq);
-        bk.launch(K_FLIP_DO, c, nq);
-        bk.read(&h); st.host_syncs++;
-        if (h.status) return h.status;
-        bk.launch(K_FLIP_FIX, c, h.n_flip);
-        st.flips += h.n_flip;
-        st.flip_subrounds++;
-        sr++;
-        nq = h.n_next;
-        int* t = qa; qa = qb; qb = t;
+        c.queue = D.qa; c.queue_next = D.qb; c.sr = D.sr;
+        c.base_q = D.e_q;
+        c.base_flip = D.e_flip;
+        run_phase(ex, c, D, K_FLIP_CHECK, nq);
+        run_phase(ex, c, D, K_FLIP_DO, nq);
+        D.e_q = ex.cursor(&c.cnt->cur_q);
+        D.e_flip = ex.cursor(&c.cnt->cur_flip);
+        if (D.errs) return D.errs;
+        run_phase(ex, c, D, K_FLIP_FIX, (long long)(D.e_flip - c.base_flip));
+        D.subrounds++;
+        D.sr++;
+        nq = (long long)(D.e_q - c.base_q);
+        int* t = D.qa; D.qa = D.qb; D.qb = t;
     }
     return 0;
 }
 
+template <class EX>
+GCDT_HD int insert_rounds(EX& ex, Ctx& c, Driver& D, long long nact) {
+    while (nact > 0) {
+        if (++D.round > kMaxRounds) return ST_ITER_LIMIT;
+        c.round = D.round;
+        c.act = D.actA; c.act_next = D.actB;
+        c.base_act = D.e_act;
+        run_phase(ex, c, D, K_RELOC_VOTE, nact);
+        D.e_act = ex.cursor(&c.cnt->cur_act);
+        if (D.errs) return D.errs;
+        nact = (long long)(D.e_act - c.base_act);
+        { int* t = D.actA; D.actA = D.actB; D.actB = t; }
+        if (nact == 0) break;
+        c.act = D.actA; c.act_next = D.actB;
+        c.base_win = D.e_win;
+        run_phase(ex, c, D, K_SPLIT, nact);
+        D.e_win = ex.cursor(&c.cnt->cur_win);
+        long long nwin = (long long)(D.e_win - c.base_win);
+        D.sr++;
+        c.sr = D.sr; c.queue_next = D.qa;
+        c.base_q = D.e_q;
+        run_phase(ex, c, D, K_FIX, nwin);
+        D.e_q = ex.cursor(&c.cnt->cur_q);
+        if (D.errs) return D.errs;
+        D.rounds++;
+        int rc = flip_until_delaunay(ex, c, D, (long long)(D.e_q - c.base_q));
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+// Recover every segment on the current (coarse) mesh, then restore the
+// constrained Delaunay property.
+template <class EX>
+GCDT_HD int insert_constraints(EX& ex, Ctx& c, Driver& D) {
+    c.level = 1;
+    run_phase(ex, c, D, K_VT_RESET, c.n + 4);
+    run_phase(ex, c, D, K_VT_LIVE, c.n + 2);
+    int* pa = c.pend;
+    int* pb = c.pend_next;
+    long long npend = c.s;
+    unsigned lawson_sr = D.sr + kMaxConstraintRounds + 2;
+    c.lawson_sr = lawson_sr;
+    c.lq = D.qa;
+    c.base_law = D.e_law;
+    unsigned cr = 0;
+    while (npend > 0) {
+        if (++cr > kMaxConstraintRounds) return ST_ITER_LIMIT;
+        D.sr++;
+        c.sr = D.sr;
+        c.pend = pa; c.pend_next = pb;
+        c.base_pend = D.e_pend;
+        c.base_scr = D.e_scr;
+        run_phase(ex, c, D, K_CWALK, npend);
+        run_phase(ex, c, D, K_CCLAIM, npend);
+        D.e_scr = ex.cursor(&c.cnt->cur_scr);
+        run_phase(ex, c, D, K_CPROC, npend);
+        D.e_pend = ex.cursor(&c.cnt->cur_pend);
+        D.e_law = ex.cursor(&c.cnt->cur_law);
+        if (D.errs) return D.errs;
+        npend = (long long)(D.e_pend - c.base_pend);
+        int* t = pa; pa = pb; pb = t;
+        D.crounds++;
+    }
+    long long nlaw = (long long)(D.e_law - c.base_law);
+    D.sr = lawson_sr;
+    return flip_until_delaunay(ex, c, D, nlaw);
+}
+
+// Everything after the sort: the insertion levels, the constraint stage
+// after level 0, and the output.  Cursors start at 0 (cleared by the host).
+template <class EX>
+GCDT_HD int run_stages(EX& ex, Ctx c) {
+    const int n = c.n;
+    Driver D;
+    D.actA = c.act; D.actB = c.act_next; D.qa = c.queue; D.qb = c.queue_next;
+    D.round = 0; D.sr = 0; D.rounds = 0; D.subrounds = 0; D.crounds = 0;
+    D.e_act0 = D.e_act = D.e_win = D.e_q = D.e_flip = D.e_pend = D.e_law = D.e_scr = 0;
+    D.nphase = 0; D.errs = 0;
+    int rc = 0;
+    for (int l = 0; l < c.nlevels && n > 0 && rc == 0; ++l) {
+        c.level = l;
+        if (l > 0) {
+            run_phase(ex, c, D, K_VT_RESET, n + 4);
+            run_phase(ex, c, D, K_VT_LIVE, n + 2);
+        }
+        c.act_next = D.actA;
+        c.base_act = D.e_act0;
+        run_phase(ex, c, D, K_ACTIVATE, n);
+        D.e_act0 = ex.cursor(&c.cnt->cur_act0);
+        if ((rc = D.errs)) break;
+        rc = insert_rounds(ex, c, D, (long long)(D.e_act0 - c.base_act));
+        if (rc == 0 && l == 0 && c.s > 0) rc = insert_constraints(ex, c, D);
+    }
+    if (rc == 0 && n == 0 && c.s > 0) rc = ST_BAD_INPUT;
+    if (rc == 0) {
+        run_phase(ex, c, D, K_OUTPUT, c.ntri);
+        rc = D.errs;
+    }
+    ex.finish(c, D.rounds, D.subrounds, D.crounds, rc | D.errs);
+    return rc;
+}
+
+// Host part: clear the per-solve arrays, Morton sort, gather, levels and
+// segment set-up, then hand over to the stages (one persistent kernel on the
+// GPU).
 template <class BK>
 int run_solve(BK& bk, Ctx c, SolveStats& st) {
-    Counters h;
     const int n = c.n;
     const long long T = c.ntri;
     bk.fill(c.cnt, 0, sizeof(Counters));
@@ -142,82 +286,21 @@ int run_solve(BK& bk, Ctx c, SolveStats& st) {
     }
     bk.launch(K_GATHER, c, n + 4);
     bk.launch(K_ROOT, c, 1);
-    if (n > 0) bk.launch(K_INITLOC, c, n);
-    bk.read(&h); st.host_syncs++;
-    if (h.status) return h.status;
-
-    // ---- phase 1: insertion rounds
-    int* actA = c.act;
-    int* actB = c.act_next;
-    int* qa = c.queue;
-    int* qb = c.queue_next;
-    int nact = n;
-    unsigned round = 0, sr = 0;
-    while (nact > 0) {
-        if (++round > kMaxRounds) return ST_ITER_LIMIT;
-        c.round = round;
-        c.act = actA; c.act_next = actB;
-        bk.reset_lists();
-        bk.launch(K_RELOC_VOTE, c, nact);
-        bk.read(&h); st.host_syncs++;
-        if (h.status) return h.status;
-        nact = h.n_next;
-        { int* t = actA; actA = actB; actB = t; }
-        if (nact == 0) break;
-        c.act = actA; c.act_next = actB;
-        bk.launch(K_SPLIT, c, nact);
-        bk.read(&h); st.host_syncs++;
-        int nwin = h.n_win;
-        sr++;
-        c.sr = sr; c.queue_next = qa;
-        bk.reset_lists();
-        bk.launch(K_FIX, c, nwin);
-        bk.read(&h); st.host_syncs++;
-        if (h.status) return h.status;
-        st.rounds++;
-        int rc = flip_until_delaunay(bk, c, qa, qb, h.n_next, sr, st);
-        if (rc) return rc;
-    }
-
-    // ---- phase 2: constraints
+    if (n > 0) bk.launch(K_LEVEL, c, n);
     if (c.s > 0) {
-        bk.launch(K_VT, c, T);
         bk.launch(K_SEG_INIT, c, c.s);
-        bk.read(&h); st.host_syncs++;
-        if (h.status) return h.status;
-        int* pa = c.pend;
-        int* pb = c.pend_next;
-        int npend = c.s;
-        unsigned lawson_sr = sr + kMaxConstraintRounds + 2;
-        c.lawson_sr = lawson_sr;
-        c.lq = qa;
-        unsigned cr = 0;
-        while (npend > 0) {
-            if (++cr > kMaxConstraintRounds) return ST_ITER_LIMIT;
-            sr++;
-            c.sr = sr;
-            c.pend = pa; c.pend_next = pb;
-            bk.reset_lists();
-            bk.set_scratch_top(0);
-            bk.launch(K_CWALK, c, npend);
-            bk.launch(K_CCLAIM, c, npend);
-            bk.launch(K_CPROC, c, npend);
-            bk.read(&h); st.host_syncs++;
-            if (h.status) return h.status;
-            npend = h.n_next;
-            int* t = pa; pa = pb; pb = t;
-            st.constraint_rounds++;
-        }
-        sr = lawson_sr;
-        int rc = flip_until_delaunay(bk, c, qa, qb, h.n_lawson, sr, st);
-        if (rc) return rc;
+        bk.launch(K_SEG_LEVEL0, c, c.s);
     }
-    c.sr = sr;
-
-    // ---- phase 3: output
-    bk.launch(K_OUTPUT, c, T);
+    Counters h;
     bk.read(&h); st.host_syncs++;
-    return h.status;
+    if (h.status | h.err[0] | h.err[1]) return h.status | h.err[0] | h.err[1];
+    bk.stages(c);
+    bk.read(&h); st.host_syncs++;
+    st.rounds = h.rounds;
+    st.flip_subrounds = h.flip_subrounds;
+    st.constraint_rounds = h.constraint_rounds;
+    st.flips = (long long)h.cur_flip;
+    return h.status | h.err[0] | h.err[1];
 }
 
 }  // namespace gcdt
