@@ -196,6 +196,7 @@ def run_ours(args):
         launches += tri.stats()["kernel_launches"]
     barrier()
     clocks = sampler.stop()
+    prof = tri.phase_profile()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ms_local = statistics.median(step_ms)
     ms = max_over_ranks(ms_local)
@@ -263,6 +264,8 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clocks,
             "solve_stats": st,
+            "phase_ms": {k: round(v[0] / ((clocks.get("sm_mhz") or 1965.0) * 1e3), 3) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "phase_runs": {k: v[1] for k, v in prof.items()},
             "step_ms": step_ms,
             "validated": valid,
         }

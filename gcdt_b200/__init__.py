@@ -78,6 +78,10 @@ def lib():
     L.gcdt_get_stats.restype = ctypes.c_int
     L.gcdt_status_string.argtypes = [ctypes.c_int]
     L.gcdt_status_string.restype = ctypes.c_char_p
+    L.gcdt_get_phase_profile.argtypes = [vp, vp, vp, i32]
+    L.gcdt_get_phase_profile.restype = i32
+    L.gcdt_phase_name.argtypes = [i32]
+    L.gcdt_phase_name.restype = ctypes.c_char_p
     L.gcdt_eval_predicates.argtypes = [vp, i32, vp, vp]
     L.gcdt_eval_predicates.restype = ctypes.c_int
     _LIB = L
@@ -210,6 +214,18 @@ class Triangulator:
             sgm = torch.from_numpy(np.ascontiguousarray(segments, dtype=np.int32)).to(dev)
         tris, adj, cflags = self.triangulate(p, sgm)
         return tris.cpu().numpy(), adj.cpu().numpy(), cflags.cpu().numpy()
+
+    def phase_profile(self):
+        """{phase name: (SM cycles, runs)} of the last solve's persistent kernel."""
+        cyc = np.zeros(32, np.int64)
+        cnt = np.zeros(32, np.int64)
+        k = lib().gcdt_get_phase_profile(self._h, ctypes.c_void_p(cyc.ctypes.data),
+                                         ctypes.c_void_p(cnt.ctypes.data), 32)
+        out = {}
+        for i in range(max(k, 0)):
+            if cnt[i]:
+                out[lib().gcdt_phase_name(i).decode()] = (int(cyc[i]), int(cnt[i]))
+        return out
 
     def stats(self):
         st = Stats()

@@ -44,8 +44,11 @@ __global__ void gcdt_predicates(const int2* q, int n, int* out) {
 constexpr int kPersistBlock = 256;
 
 struct GridExec {
+    static constexpr bool kCanNarrow = true;
     Counters* cnt;
     unsigned nblocks;
+    __device__ int narrow_flips(Ctx& c, Driver& D, long long& nq);
+    __device__ int narrow_rounds(Ctx& c, Driver& D, long long nact);
 
     // Sense-free generation barrier.  Every wait is bounded: after ~2^24
     // polls the block records ST_BARRIER and stops waiting, and once that bit
@@ -77,12 +80,18 @@ struct GridExec {
         __syncthreads();
     }
     __device__ void phase(int k, const Ctx& c, long long count) {
+        const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+        long long t0 = timer ? clock64() : 0;
         if (!(word(&cnt->status) & ST_BARRIER)) {
             long long stride = (long long)gridDim.x * blockDim.x;
             for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
                 dispatch(k, c, (int)i);
         }
         barrier();
+        if (timer && k < kMaxPhaseKinds) {   // phase time incl. the barrier, as block 0 sees it
+            cnt->phase_cyc[k] += clock64() - t0;
+            cnt->phase_cnt[k] += 1;
+        }
     }
     __device__ unsigned long long cursor(unsigned long long* p) { return *(volatile unsigned long long*)p; }
     __device__ int word(int* p) { return *(volatile int*)p; }
@@ -95,6 +104,74 @@ struct GridExec {
         }
     }
 };
+
+// Executor of one block: a phase is a block-stride loop and a block barrier.
+// Used by block 0 for the short tails while the other blocks wait.
+struct BlockExec {
+    static constexpr bool kCanNarrow = false;
+    Counters* cnt;
+    __device__ void phase(int k, const Ctx& c, long long count) {
+        for (long long i = threadIdx.x; i < count; i += blockDim.x) dispatch(k, c, (int)i);
+        __syncthreads();
+    }
+    __device__ unsigned long long cursor(unsigned long long* p) { return *(volatile unsigned long long*)p; }
+    __device__ int word(int* p) { return *(volatile int*)p; }
+    __device__ void finish(const Ctx&, long long, long long, long long, int) {}
+    __device__ int narrow_flips(Ctx&, Driver&, long long&) { return ST_INTERNAL; }
+    __device__ int narrow_rounds(Ctx&, Driver&, long long) { return ST_INTERNAL; }
+};
+
+static_assert(sizeof(Driver) <= sizeof(((Counters*)0)->handoff), "driver state fits the hand-off area");
+static_assert(sizeof(Driver) % 8 == 0, "driver state is whole 8-byte words");
+
+__device__ void store_handoff(Counters* cnt, const Driver& D, long long nq, int rc) {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&D);
+    for (unsigned k = 0; k < sizeof(Driver) / 8; ++k) cnt->handoff[k] = src[k];
+    cnt->handoff_nq = nq;
+    cnt->handoff_rc = rc;
+}
+
+__device__ int load_handoff(Counters* cnt, Driver& D, long long& nq) {
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&D);
+    volatile unsigned long long* src = cnt->handoff;
+    for (unsigned k = 0; k < sizeof(Driver) / 8; ++k) dst[k] = src[k];
+    nq = *(volatile long long*)&cnt->handoff_nq;
+    return *(volatile int*)&cnt->handoff_rc;
+}
+
+__device__ int GridExec::narrow_flips(Ctx& c, Driver& D, long long& nq) {
+    const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+    long long t0 = timer ? clock64() : 0;
+    if (blockIdx.x == 0) {
+        BlockExec bx{cnt};
+        Driver Db = D;
+        Ctx cb = c;
+        long long left = nq;
+        int rc = flip_loop(bx, cb, Db, left, 4 * kNarrowQueue);
+        if (threadIdx.x == 0) store_handoff(cnt, Db, left, rc);
+    }
+    barrier();
+    int rc = load_handoff(cnt, D, nq);
+    if (timer) { cnt->phase_cyc[K_NARROW_FLIPS] += clock64() - t0; cnt->phase_cnt[K_NARROW_FLIPS] += 1; }
+    return rc;
+}
+
+__device__ int GridExec::narrow_rounds(Ctx& c, Driver& D, long long nact) {
+    const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+    long long t0 = timer ? clock64() : 0;
+    if (blockIdx.x == 0) {
+        BlockExec bx{cnt};
+        Driver Db = D;
+        Ctx cb = c;
+        int rc = insert_rounds(bx, cb, Db, nact);
+        if (threadIdx.x == 0) store_handoff(cnt, Db, 0, rc);
+    }
+    barrier();
+    long long dummy;
+    int rc = load_handoff(cnt, D, dummy);
+    if (timer) { cnt->phase_cyc[K_NARROW_ROUNDS] += clock64() - t0; cnt->phase_cnt[K_NARROW_ROUNDS] += 1; }
+    return rc;
+}
 
 __global__ void __launch_bounds__(kPersistBlock, 2) gcdt_stages(Ctx c) {
     GridExec ex{c.cnt, gridDim.x};
@@ -408,4 +485,26 @@ extern "C" gcdt_status gcdt_triangulate_noalloc(const int32_t* d_points, int32_t
     gcdt_status rc = map_status(bits);
     if (rc == GCDT_OK && n_tris) *n_tris = 2 * n + 2;
     return rc;
+}
+
+static const char* const kPhaseNames[] = {
+    "keys", "gather", "root", "level", "seg_level0", "activate", "vt_reset", "vt_live",
+    "reloc_vote", "split", "fix", "flip_check", "flip_do", "flip_fix", "output",
+    "seg_init", "cwalk", "cclaim", "cproc", "narrow_flips", "narrow_rounds"};
+static_assert(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]) == K_COUNT, "one name per phase kind");
+
+extern "C" int32_t gcdt_get_phase_profile(const gcdt_context* ctx, int64_t* cycles, int64_t* counts, int32_t max_kinds) {
+    if (!ctx || !ctx->hcnt || max_kinds < 0) return -1;
+    int32_t n = (int32_t)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
+    if (n > kMaxPhaseKinds) n = kMaxPhaseKinds;
+    for (int32_t k = 0; k < n && k < max_kinds; ++k) {
+        if (cycles) cycles[k] = ctx->hcnt->phase_cyc[k];
+        if (counts) counts[k] = ctx->hcnt->phase_cnt[k];
+    }
+    return n;
+}
+
+extern "C" const char* gcdt_phase_name(int32_t kind) {
+    int32_t n = (int32_t)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
+    return (kind >= 0 && kind < n) ? kPhaseNames[kind] : "";
 }

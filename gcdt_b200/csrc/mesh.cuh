@@ -34,6 +34,7 @@
 namespace gcdt {
 
 constexpr int kBoxMax = (1 << 30) - 1;   // R = 2^30 - 1
+constexpr int kMaxPhaseKinds = 24;
 
 enum StatusBits : int {
     ST_OK = 0,
@@ -64,6 +65,12 @@ struct Counters {
     unsigned int bar_gen;
     long long rounds, flip_subrounds, constraint_rounds;
     long long pad1[3];
+    long long phase_cyc[kMaxPhaseKinds];   // SM cycles per phase kind (block 0's view)
+    long long phase_cnt[kMaxPhaseKinds];
+    unsigned long long handoff[24];        // driver state handed back by a single-block tail
+    long long handoff_nq;
+    int handoff_rc;
+    int pad2;
 };
 
 struct Ctx {
@@ -504,9 +511,10 @@ GCDT_HD int split_child(int2 im, int m, int ms) {
     return ms == nx3(e) ? m : 3 + 2 * qm;
 }
 
+// The children of the inserted points are distinct triangles, so the first
+// flip queue of a round needs no de-duplication.
 GCDT_HD void push_queue(const Ctx& c, int t) {
-    if (at_exch(&c.qst[t], (int)c.sr) != (int)c.sr)
-        c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = t;
+    c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = t;
 }
 
 GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
@@ -577,19 +585,17 @@ GCDT_HD void body_flip_check(const Ctx& c, int k) {
 }
 
 // Winners flip: t=(A,B,C) with A in slot i, n=(D,C,B) with D in slot j
-// become t=(A,B,D), n=(A,D,C).  Losers are re-queued.
+// become t=(A,B,D), n=(A,D,C), and both go to the next queue.  Losers are
+// re-queued by body_flip_fix once it is known that nobody flipped them, so
+// every triangle enters the next queue at most once without any
+// de-duplication.
 GCDT_HD void body_flip_do(const Ctx& c, int k) {
     int2 cd = c.cand[k];
     if (cd.x < 0) return;
     int t = cd.x >> 2, i = cd.x & 3;
     int n = cd.y >> 2, j = cd.y & 3;
     unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)cd.x));
-    if (c.claim[t] != ck || c.claim[n] != ck) {
-        // re-check next sub-round; stamp sr+1 is the next queue's stamp
-        if (at_exch(&c.qst[t], (int)c.sr + 1) != (int)c.sr + 1)
-            c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = t;
-        return;
-    }
+    if (c.claim[t] != ck || c.claim[n] != ck) return;
     int4 tv = c.TV[t], ta = c.TA[t], nv = c.TV[n], na = c.TA[n];
     int i1 = nx3(i), i2 = nx3(i1), j1 = nx3(j), j2 = nx3(j1);
     int A = comp(tv, i), B = comp(tv, i1), C = comp(tv, i2), D = comp(nv, j);
@@ -608,10 +614,9 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     c.modR[t] = (int)c.round;
     c.modR[n] = (int)c.round;
     c.flipped[append_slot(&c.cnt->cur_flip, c.base_flip)] = t;
-    if (at_exch(&c.qst[t], (int)c.sr + 1) != (int)c.sr + 1)
-        c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = t;
-    if (at_exch(&c.qst[n], (int)c.sr + 1) != (int)c.sr + 1)
-        c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = n;
+    int qi = append_slot(&c.cnt->cur_q, c.base_q);
+    c.queue_next[qi] = t;
+    c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = n;
 }
 
 GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
@@ -626,7 +631,16 @@ GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
     }
 }
 
+// k < c.list_n: resolve the outer adjacency of flipped pair k.
+// Otherwise queue entry k - c.list_n: a candidate that did not flip and
+// whose triangle nobody flipped goes back to the queue.
 GCDT_HD void body_flip_fix(const Ctx& c, int k) {
+    if (k >= c.list_n) {
+        int2 cd = c.cand[k - c.list_n];
+        if (cd.x >= 0 && c.fst[cd.x >> 2] != (int)c.sr)
+            c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = cd.x >> 2;
+        return;
+    }
     int t = c.flipped[k];
     int n = c.TA[t].y >> 2;
     resolve_flip_edge(c, t, 0);

@@ -23,6 +23,7 @@ enum Kern : int {
     K_RELOC_VOTE, K_SPLIT, K_FIX,
     K_FLIP_CHECK, K_FLIP_DO, K_FLIP_FIX, K_OUTPUT,
     K_SEG_INIT, K_CWALK, K_CCLAIM, K_CPROC,
+    K_NARROW_FLIPS, K_NARROW_ROUNDS,     // timing labels of the single-block tails
     K_COUNT
 };
 
@@ -106,6 +107,10 @@ GCDT_HD void dispatch(int k, const Ctx& c, int i) {
 }
 
 constexpr long long kMaxSubrounds = 1 << 20;
+// A flip queue or an active list this short is finished by one block with
+// block barriers instead of the whole grid with grid barriers.
+constexpr long long kNarrowQueue = 1024;
+constexpr long long kNarrowActive = 1024;
 constexpr long long kMaxRounds = 1 << 16;
 constexpr unsigned kMaxConstraintRounds = 1 << 14;
 
@@ -121,7 +126,9 @@ constexpr unsigned kMaxConstraintRounds = 1 << 14;
 //     while phase k+1 writes err[(k+1) & 1].
 //
 // EX provides: phase(kernel, ctx, count), cursor(u64*) -> u64,
-// word(int*) -> int, finish(...).
+// word(int*) -> int, finish(...), and kCanNarrow: whether small flip queues
+// and small insertion tails can be handed to one block (narrow_flips,
+// narrow_rounds), which runs this same driver with block barriers.
 
 struct Driver {
     int* actA; int* actB; int* qa; int* qb;
@@ -140,21 +147,29 @@ GCDT_HD void run_phase(EX& ex, Ctx& c, Driver& D, int k, long long count) {
     D.nphase++;
 }
 
-// Flip sub-rounds until the queue `D.qa` (nq entries, stamped D.sr) is empty.
+// Flip sub-rounds until the queue `D.qa` (nq entries, stamped D.sr) is
+// empty, or -- for the single-block tail -- until it grows past max_nq.
 template <class EX>
-GCDT_HD int flip_until_delaunay(EX& ex, Ctx& c, Driver& D, long long nq) {
+GCDT_HD int flip_loop(EX& ex, Ctx& c, Driver& D, long long& nq, long long max_nq) {
     long long guard = 0;
-    while (nq > 0) {
+    while (nq > 0 && nq <= max_nq) {
         if (++guard > kMaxSubrounds) return ST_ITER_LIMIT;
+        if (EX::kCanNarrow && nq <= kNarrowQueue) {
+            int rc = ex.narrow_flips(c, D, nq);
+            if (rc || D.errs) return rc ? rc : D.errs;
+            continue;
+        }
         c.queue = D.qa; c.queue_next = D.qb; c.sr = D.sr;
         c.base_q = D.e_q;
         c.base_flip = D.e_flip;
         run_phase(ex, c, D, K_FLIP_CHECK, nq);
         run_phase(ex, c, D, K_FLIP_DO, nq);
-        D.e_q = ex.cursor(&c.cnt->cur_q);
         D.e_flip = ex.cursor(&c.cnt->cur_flip);
         if (D.errs) return D.errs;
-        run_phase(ex, c, D, K_FLIP_FIX, (long long)(D.e_flip - c.base_flip));
+        long long nflip = (long long)(D.e_flip - c.base_flip);
+        c.list_n = (int)nflip;
+        run_phase(ex, c, D, K_FLIP_FIX, nflip + nq);   // FLIP_DO and FLIP_FIX both append the next queue
+        D.e_q = ex.cursor(&c.cnt->cur_q);
         D.subrounds++;
         D.sr++;
         nq = (long long)(D.e_q - c.base_q);
@@ -164,8 +179,14 @@ GCDT_HD int flip_until_delaunay(EX& ex, Ctx& c, Driver& D, long long nq) {
 }
 
 template <class EX>
+GCDT_HD int flip_until_delaunay(EX& ex, Ctx& c, Driver& D, long long nq) {
+    return flip_loop(ex, c, D, nq, (long long)1 << 62);
+}
+
+template <class EX>
 GCDT_HD int insert_rounds(EX& ex, Ctx& c, Driver& D, long long nact) {
     while (nact > 0) {
+        if (EX::kCanNarrow && nact <= kNarrowActive) return ex.narrow_rounds(c, D, nact);
         if (++D.round > kMaxRounds) return ST_ITER_LIMIT;
         c.round = D.round;
         c.act = D.actA; c.act_next = D.actB;

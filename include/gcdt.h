@@ -88,6 +88,14 @@ gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_points, int32_t
 gcdt_status gcdt_get_stats(const gcdt_context* ctx, gcdt_stats* out);
 const char* gcdt_status_string(gcdt_status s);
 
+/* Per-phase profile of the last solve on ctx: SM cycles spent in each phase
+   kind of the persistent stage kernel (measured by block 0, barrier wait
+   included) and how often it ran.  Returns the number of phase kinds
+   (names: gcdt_phase_name), or -1 on bad arguments.  Counters of the
+   reference's per-stage cudaEvent printouts (e.g. rawMesh.cu:1008-1031). */
+int32_t gcdt_get_phase_profile(const gcdt_context* ctx, int64_t* cycles, int64_t* counts, int32_t max_kinds);
+const char* gcdt_phase_name(int32_t kind);
+
 /* Exact predicates on device, for parity tests.  d_quads: 8 int32 per case
    (a, b, c, d points); d_out: 3 int32 per case = orient2d(a,b,c),
    inCircle(a,b,c,d) (exact sign, math_base.cuh:267-328) and the perturbed
