@@ -511,10 +511,15 @@ GCDT_HD int split_child(int2 im, int m, int ms) {
     return ms == nx3(e) ? m : 3 + 2 * qm;
 }
 
+// Flip-queue entry: triangle id << 3 | mask of the slots whose edges may
+// not be locally Delaunay (the others are known to be).
+GCDT_HD int qentry(int t, int mask) { return (int)(((unsigned)t << 3) | (unsigned)mask); }
+GCDT_HD int qtri(int e) { return (int)((unsigned)e >> 3); }
+
 // The children of the inserted points are distinct triangles, so the first
 // flip queue of a round needs no de-duplication.
-GCDT_HD void push_queue(const Ctx& c, int t) {
-    c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = t;
+GCDT_HD void push_queue(const Ctx& c, int t, int mask) {
+    c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = qentry(t, mask);
 }
 
 GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
@@ -537,11 +542,15 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
     int q = w.x, t = w.y;
     int T1 = 2 + 2 * q, T2 = 3 + 2 * q;
     int code = c.ins[t].y & 7;
+    // Only the old edges need a test: a spoke from q to a corner of the split
+    // triangle is locally Delaunay (q lies inside the old empty circumcircle,
+    // so the circle through q and the spoke's far edge excludes the third
+    // corner; on an edge split the spoke's quadrilateral is not even convex).
     if (code == 7) {
         resolve_split_edge(c, t, 0);
         resolve_split_edge(c, T1, 1);
         resolve_split_edge(c, T2, 2);
-        push_queue(c, t); push_queue(c, T1); push_queue(c, T2);
+        push_queue(c, t, 1); push_queue(c, T1, 2); push_queue(c, T2, 4);
     } else {
         int e = code;
         int e1 = nx3(e), e_2 = nx3(e1);
@@ -552,7 +561,9 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
         resolve_split_edge(c, T1, e_2);
         resolve_split_edge(c, n, f1);
         resolve_split_edge(c, T2, f2);
-        push_queue(c, t); push_queue(c, T1); push_queue(c, n); push_queue(c, T2);
+        // outer edge and the half of the split edge
+        push_queue(c, t, (1 << e1) | (1 << e)); push_queue(c, T1, (1 << e_2) | (1 << e));
+        push_queue(c, n, (1 << f1) | (1 << e2)); push_queue(c, T2, (1 << f2) | (1 << e2));
     }
 }
 
@@ -564,10 +575,12 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
 // smallest wins both triangles (atomicMax of its complement), so conflicts
 // resolve like a random-priority independent set, whatever the schedule.
 GCDT_HD void body_flip_check(const Ctx& c, int k) {
-    int t = c.queue[k];
+    int qe = c.queue[k];
+    int t = qtri(qe), mask = qe & 7;
     int4 tv = c.TV[t], ta = c.TA[t];
     int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
     for (int i = 0; i < 3; ++i) {
+        if (!((mask >> i) & 1)) continue;
         int en = comp(ta, i);
         if (en < 0 || ((tv.w >> i) & 1)) continue;
         int n = en >> 2, j = en & 3;
@@ -614,9 +627,10 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     c.modR[t] = (int)c.round;
     c.modR[n] = (int)c.round;
     c.flipped[append_slot(&c.cnt->cur_flip, c.base_flip)] = t;
+    // the new diagonal AD is locally Delaunay: queue the four outer edges
     int qi = append_slot(&c.cnt->cur_q, c.base_q);
-    c.queue_next[qi] = t;
-    c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = n;
+    c.queue_next[qi] = qentry(t, 5);    // (A,B,D): BD and AB
+    c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = qentry(n, 3);   // (A,D,C): DC and CA
 }
 
 GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
@@ -638,7 +652,7 @@ GCDT_HD void body_flip_fix(const Ctx& c, int k) {
     if (k >= c.list_n) {
         int2 cd = c.cand[k - c.list_n];
         if (cd.x >= 0 && c.fst[cd.x >> 2] != (int)c.sr)
-            c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = cd.x >> 2;
+            c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = c.queue[k - c.list_n];
         return;
     }
     int t = c.flipped[k];
@@ -805,7 +819,7 @@ GCDT_HD int flip_local(const Ctx& c, int t, int i) {
 
 GCDT_HD void push_lawson(const Ctx& c, int t) {
     if (at_exch(&c.qst[t], (int)c.lawson_sr) != (int)c.lawson_sr)
-        c.lq[append_slot(&c.cnt->cur_law, c.base_law)] = t;
+        c.lq[append_slot(&c.cnt->cur_law, c.base_law)] = qentry(t, 7);
 }
 
 // Owners of all their triangles recover the sub-segment (a, stop) by

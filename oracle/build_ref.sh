@@ -1,0 +1,62 @@
+#!/usr/bin/env bash
+# Build the reference's own CUDA pipeline (yingtix/gCDT) for sm_100a, linked
+# with oracle/ref_harness.cu, into oracle/_ref/gcdt_ref.
+#
+# TEST INFRASTRUCTURE ONLY: the binary is a checker and a comparison point;
+# the product never links or runs it.
+#
+# The reference is MSVC code and needs six mechanical portability patches.
+# They are applied to a throw-away copy under /tmp (the reference tree is
+# read-only and no reference source enters this repository):
+#   1. include/MemCache.h       add the standard headers it uses
+#   2. MemCache.cpp             "memCache.h" -> "MemCache.h" (case-sensitive fs)
+#   3. include/math_base.cuh    `unsigned int(x)` -> `(unsigned int)(x)`
+#   4. include/{rawMesh,boostmap,addConstraints,fastDelaunay}.h
+#                               `typename Point2d;` -> `typedef int2 Point2d;`
+#   5. kernel.cu                `return;` at the end of main -> `return 0;`
+#   6. utils.cu                 drop six duplicate RKERNEL explicit instantiations
+# kernel.cu is compiled with -Dmain=gcdt_ref_unused_main; the harness
+# supplies main.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${GCDT_REFERENCE_DIR:-/root/reference}"
+OUT="$HERE/_ref"
+WORK="$(mktemp -d /tmp/gcdt_ref_src.XXXXXX)"
+trap 'rm -rf "$WORK"' EXIT
+
+if [ ! -f "$REF/kernel.cu" ]; then
+    echo "reference sources not found at $REF" >&2
+    exit 1
+fi
+cp -r "$REF"/. "$WORK"/
+chmod -R u+w "$WORK"
+cd "$WORK"
+
+# 1
+sed -i '1a #include <list>\n#include <vector>\n#include <algorithm>\n#include <cstdio>' include/MemCache.h
+# 2
+sed -i 's/#include "memCache.h"/#include "MemCache.h"/' MemCache.cpp
+# 3
+sed -i 's/unsigned int(c \& 0xFFFFFFFF), unsigned int(c >> 32)/(unsigned int)(c \& 0xFFFFFFFF), (unsigned int)(c >> 32)/' include/math_base.cuh
+# 4
+for h in rawMesh boostmap addConstraints fastDelaunay; do
+    sed -i 's/^typename Point2d;/#include <vector_types.h>\ntypedef int2 Point2d;/' "include/$h.h"
+done
+# 5
+sed -i '5465s/^\treturn;$/\treturn 0;/' kernel.cu
+# 6 (highest line first so the numbers stay valid)
+for l in 467 462 461 457 432 401; do
+    if grep -q '^RKERNEL' <(sed -n "${l}p" utils.cu); then sed -i "${l}d" utils.cu; fi
+done
+
+NVCC="${NVCC:-nvcc}"
+FLAGS=(-std=c++14 -O3 --expt-relaxed-constexpr -rdc=true -gencode arch=compute_100a,code=sm_100a -Iinclude -w)
+mkdir -p "$OUT" objs
+for f in rawMesh.cu boostmap.cu addConstraints.cu utils.cu fastDelaunay.cu; do
+    "$NVCC" "${FLAGS[@]}" -c "$f" -o "objs/${f%.cu}.o"
+done
+"$NVCC" "${FLAGS[@]}" -Dmain=gcdt_ref_unused_main -c kernel.cu -o objs/kernel.o
+"$NVCC" "${FLAGS[@]}" -x cu -c MemCache.cpp -o objs/MemCache.o
+"$NVCC" "${FLAGS[@]}" -c "$HERE/ref_harness.cu" -o objs/ref_harness.o
+"$NVCC" -gencode arch=compute_100a,code=sm_100a -rdc=true objs/*.o -o "$OUT/gcdt_ref"
+echo "built $OUT/gcdt_ref"
