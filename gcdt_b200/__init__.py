@@ -106,7 +106,7 @@ def _gen_lib():
 
 
 # Workload kinds of gcdt_gen_new (see gcdt_b200/csrc/gen.cpp).
-GEN_SMALL, GEN_SCALE, GEN_LATTICE, GEN_BATCH_INSTANCE, GEN_SERVING_REQUEST = 0, 1, 2, 3, 4
+GEN_SMALL, GEN_SCALE, GEN_LATTICE, GEN_BATCH_INSTANCE, GEN_SERVING_REQUEST, GEN_UNIFORM = 0, 1, 2, 3, 4, 5
 
 
 def generate(kind, seed, a=0, b=0, c=0, d=0):

@@ -257,6 +257,8 @@ extern "C" {
 //     in distinct quadrants
 //  4  one serving request: config-1 mix scaled to [1, 2^28), stars totalling
 //     about 2% of the point count
+//  5  uniform points over the whole box [1, 2^30-2]^2 (the distribution of the
+//     reference driver's own randomMap, kernel.cu:43-58), no segments
 // Parameters a,b,c,d are kind specific (0 = default).
 void* gcdt_gen_new(int kind, uint64_t seed, int64_t a, int64_t b, int64_t c, int64_t d) {
     Instance* I = new Instance();
@@ -313,6 +315,12 @@ void* gcdt_gen_new(int kind, uint64_t seed, int64_t a, int64_t b, int64_t c, int
         int G = int(std::ceil(std::sqrt(double(npoly) * 1.0)));
         gen_mixture(*I, rng, npts, (int64_t(1) << 28) - 1, 0.9, 64, double(int64_t(1) << 20),
                     int64_t(1) << 28, G, npoly, 64, 64, 0.45);
+        break;
+    }
+    case 5: {  // uniform points over the whole box [1, 2^30-2]^2, no segments
+        int64_t npts = a ? a : 1000000;
+        I->index.reserve(size_t(npts) * 2);
+        for (int64_t i = 0; i < npts; ++i) I->add_point(rng.range(1, kBoxMax), rng.range(1, kBoxMax));
         break;
     }
     default:

@@ -1,0 +1,71 @@
+"""Regenerate tests/golden/reference_fixtures.json from the reference itself.
+
+TEST INFRASTRUCTURE ONLY.  Needs a GPU and oracle/_ref/gcdt_ref (built by
+oracle/build_ref.sh from the reference sources).  For each seeded input it
+runs the reference's own device pipeline (kernel.cu:5398-5443), maps its
+triangles to input indices by coordinates and records the SHA-256 of the
+canonical triangle set, the triangle count, the reference's final Delaunay
+self-check count (`mark`, kernel.cu:4839-4844) and the number of constraints
+it ignored (`sum ig`, addConstraints.cu:1744-1751).  A case pins parity only
+where the reference's output is complete: mark == 0, nothing ignored and
+2n+2 triangles ("pinned": true).
+
+    CUDA_MODULE_LOADING=EAGER python oracle/make_reference_fixtures.py
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, ROOT)
+
+import gcdt_b200 as g  # noqa: E402
+from oracle import reference  # noqa: E402
+
+CASES = [
+    # name, generator kind, seed, args, drop segments
+    ("uniform_200k", g.GEN_UNIFORM, 13159, [200000], False),
+    ("uniform_1m", g.GEN_UNIFORM, 13159, [1000000], False),
+    ("uniform_9m", g.GEN_UNIFORM, 13159, [9000000], False),
+    ("scale_points_10m", g.GEN_SCALE, 1, [], True),
+    ("scale_10m_200k_segments", g.GEN_SCALE, 1, [], False),
+    ("small_100k_512_segments", g.GEN_SMALL, 1, [], False),
+]
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.int64).tobytes()).hexdigest()
+
+
+def main():
+    os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
+    out = {"reference": "yingtix/gCDT device pipeline, kernel.cu:5398-5443, built by oracle/build_ref.sh",
+           "cases": []}
+    for name, kind, seed, args, drop in CASES:
+        xy, cons = g.generate(kind, seed, *args)
+        if drop:
+            cons = cons[:0]
+        r = reference.run(xy, cons, repeat=1, timeout=1800)
+        T = len(r["tris"])
+        mark = r["marks"][-1] if r["marks"] else None
+        ignored = r["ignored"][-1] if r["ignored"] else 0
+        case = {"name": name, "kind": kind, "seed": seed, "args": args, "drop_segments": drop,
+                "n": int(len(xy)), "s": int(len(cons)), "input_sha256": sha(xy),
+                "ref_ntri": T, "ref_mark": mark, "ref_ignored": ignored, "ref_event_ms": r["event_ms"],
+                "ref_sum_time_ms": r["sum_time"],
+                "pinned": bool(mark == 0 and ignored == 0 and T == 2 * len(xy) + 2),
+                "tris_sha256": sha(g.canonical(r["tris"]))}
+        out["cases"].append(case)
+        print(json.dumps(case), flush=True)
+    path = os.path.join(ROOT, "tests", "golden", "reference_fixtures.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", path)
+
+
+if __name__ == "__main__":
+    main()
