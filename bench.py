@@ -155,7 +155,12 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     # replicas: rank r triangulates its own seeded instance of the workload
-    xy, cons = g.generate(g.GEN_SCALE, 1 + rank)
+    if args.scale_points:
+        # reduced copy of the workload shape, for profiling runs only
+        gsz = max(2, int(round(56 * (args.scale_points / 10_000_000) ** 0.5)))
+        xy, cons = g.generate(g.GEN_SCALE, 1 + rank, args.scale_points, gsz, int(gsz * gsz * 3125 / 3136))
+    else:
+        xy, cons = g.generate(g.GEN_SCALE, 1 + rank)
     n, s = len(xy), len(cons)
     tri = g.Triangulator(max_points=n, max_segments=s, device=local)
     stream = torch.cuda.current_stream(dev)
@@ -251,7 +256,8 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "i64/i128 exact predicates on i32 coordinates (f64 filter)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_points": n, "n_segments": s, "n_triangles": T,
+            "config": {"workload": WORKLOAD if not args.scale_points else "PROFILING ONLY, reduced: %d generated points" % args.scale_points,
+                       "n_points": n, "n_segments": s, "n_triangles": T,
                        "parallelism": "replicas (one independent triangulation per GPU)" if world > 1 else "single GPU",
                        "l2": "256 MB buffer written between timed steps; working set ~2 GB"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -285,6 +291,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-repeat", type=int, default=3)
     ap.add_argument("--validate", action="store_true")
+    ap.add_argument("--scale-points", type=int, default=0,
+                    help="profiling only: a reduced copy of the workload with this many generated points")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per solve from an ncu capture, reported as roofline.traffic")
     args = ap.parse_args()
