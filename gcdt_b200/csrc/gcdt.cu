@@ -3,6 +3,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cstdio>
 #include <cstring>
+#include <cstddef>
 #include <mutex>
 #include <new>
 
@@ -50,6 +51,18 @@ struct GridExec {
     __device__ int narrow_flips(Ctx& c, Driver& D, long long& nq);
     __device__ int narrow_rounds(Ctx& c, Driver& D, long long nact);
 
+    // Snapshot of the head of Counters (status, error words, list cursors)
+    // taken by thread 0 right after each grid barrier: the driver's reads of
+    // these values come from shared memory instead of every thread reading
+    // the same L2 line.
+    static constexpr int kSnapWords = 12;   // 96 bytes: status..cur_scr
+    unsigned long long* snap;                // shared memory, kSnapWords entries
+
+    __device__ void take_snapshot() {
+        volatile unsigned long long* src = reinterpret_cast<volatile unsigned long long*>(cnt);
+        for (int k = 0; k < kSnapWords; ++k) snap[k] = src[k];
+    }
+
     // Sense-free generation barrier.  Every wait is bounded: after ~2^24
     // polls the block records ST_BARRIER and stops waiting, and once that bit
     // is set no block waits or works any more, so the kernel always ends.
@@ -76,6 +89,7 @@ struct GridExec {
                 }
             }
             __threadfence();
+            take_snapshot();
         }
         __syncthreads();
     }
@@ -93,8 +107,17 @@ struct GridExec {
             cnt->phase_cnt[k] += 1;
         }
     }
-    __device__ unsigned long long cursor(unsigned long long* p) { return *(volatile unsigned long long*)p; }
-    __device__ int word(int* p) { return *(volatile int*)p; }
+    // Values read after a barrier come from the block's snapshot.
+    __device__ unsigned long long cursor(unsigned long long* p) {
+        size_t off = (size_t)((char*)p - (char*)cnt);
+        if (off + 8 <= kSnapWords * 8) return *reinterpret_cast<unsigned long long*>((char*)snap + off);
+        return *(volatile unsigned long long*)p;
+    }
+    __device__ int word(int* p) {
+        size_t off = (size_t)((char*)p - (char*)cnt);
+        if (off + 4 <= kSnapWords * 8) return *reinterpret_cast<int*>((char*)snap + off);
+        return *(volatile int*)p;
+    }
     __device__ void finish(const Ctx&, long long rounds, long long subrounds, long long crounds, int rc) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             cnt->rounds = rounds;
@@ -173,8 +196,13 @@ __device__ int GridExec::narrow_rounds(Ctx& c, Driver& D, long long nact) {
     return rc;
 }
 
+static_assert(offsetof(Counters, cur_scr) + 8 <= GridExec::kSnapWords * 8, "cursors are in the snapshot");
+
 __global__ void __launch_bounds__(kPersistBlock, 2) gcdt_stages(Ctx c) {
-    GridExec ex{c.cnt, gridDim.x};
+    __shared__ unsigned long long snap[GridExec::kSnapWords];
+    GridExec ex{c.cnt, gridDim.x, snap};
+    if (threadIdx.x == 0) ex.take_snapshot();
+    __syncthreads();
     run_stages(ex, c);
 }
 
