@@ -82,6 +82,20 @@ def lib():
     L.gcdt_get_phase_profile.restype = i32
     L.gcdt_phase_name.argtypes = [i32]
     L.gcdt_phase_name.restype = ctypes.c_char_p
+    L.gcdt_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, i64, i64, i64]
+    L.gcdt_batch_create.restype = ctypes.c_int
+    L.gcdt_batch_destroy.argtypes = [vp]
+    L.gcdt_batch_destroy.restype = None
+    L.gcdt_batch_triangulate.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.gcdt_batch_triangulate.restype = ctypes.c_int
+    L.gcdt_batch_autotune.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]
+    L.gcdt_batch_autotune.restype = ctypes.c_int
+    L.gcdt_batch_set_config.argtypes = [vp, vp]
+    L.gcdt_batch_set_config.restype = ctypes.c_int
+    L.gcdt_batch_get_config.argtypes = [vp, vp]
+    L.gcdt_batch_get_config.restype = ctypes.c_int
+    L.gcdt_batch_last_ms.argtypes = [vp]
+    L.gcdt_batch_last_ms.restype = ctypes.c_double
     L.gcdt_eval_predicates.argtypes = [vp, i32, vp, vp]
     L.gcdt_eval_predicates.restype = ctypes.c_int
     _LIB = L
@@ -247,3 +261,123 @@ def eval_predicates(quads):
     if rc != 0:
         raise GcdtError(rc, "gcdt_eval_predicates")
     return out.cpu().numpy()
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("threads_per_instance", ctypes.c_int32), ("sample_stride", ctypes.c_int32)]
+
+
+class BatchTriangulator:
+    """Many independent triangulations per call (gcdt_batch_* in include/gcdt.h).
+
+    Instance i's output is exactly the single solve's: 2n_i+2 triangles with
+    local vertex ids and local adjacency, stored at triangle 2*P_i + 2*i of
+    the concatenated output (P_i = the instance's first point)."""
+
+    def __init__(self, max_instances, max_total_points, max_total_segments=0, device=0):
+        h = ctypes.c_void_p()
+        rc = lib().gcdt_batch_create(ctypes.byref(h), int(device), int(max_instances),
+                                     int(max_total_points), int(max_total_segments))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_batch_create")
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().gcdt_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def offsets(instances):
+        po = np.zeros(len(instances) + 1, np.int64)
+        so = np.zeros(len(instances) + 1, np.int64)
+        for i, (xy, cons) in enumerate(instances):
+            po[i + 1] = po[i] + len(xy)
+            so[i + 1] = so[i] + (0 if cons is None else len(cons))
+        return po, so
+
+    def _args(self, d_points, d_segments, po, so, out):
+        tris, adj, cflags = out
+        return (ctypes.c_void_p(po.ctypes.data), ctypes.c_void_p(so.ctypes.data),
+                ctypes.c_void_p(d_points.data_ptr() if d_points is not None and d_points.numel() else 0),
+                ctypes.c_void_p(d_segments.data_ptr() if d_segments is not None and d_segments.numel() else 0),
+                ctypes.c_void_p(tris.data_ptr()), ctypes.c_void_p(adj.data_ptr()), ctypes.c_void_p(cflags.data_ptr()))
+
+    def alloc_outputs(self, po):
+        import torch
+        ntri = int(2 * po[-1] + 2 * (len(po) - 1))
+        dev = torch.device("cuda", self.device)
+        return (torch.empty((max(ntri, 1), 3), dtype=torch.int32, device=dev),
+                torch.empty((max(ntri, 1), 3), dtype=torch.int32, device=dev),
+                torch.empty((max(ntri, 1),), dtype=torch.uint8, device=dev))
+
+    def triangulate_device(self, d_points, d_segments, po, so, out=None, stream=None):
+        """Device inputs (concatenated) -> device outputs + per-instance status codes."""
+        import torch
+        po = np.ascontiguousarray(po, np.int64)
+        so = np.ascontiguousarray(so, np.int64)
+        if out is None:
+            out = self.alloc_outputs(po)
+        st = np.zeros(len(po) - 1, np.int32)
+        if stream is None:
+            stream = torch.cuda.current_stream(torch.device("cuda", self.device)).cuda_stream
+        rc = lib().gcdt_batch_triangulate(self._h, len(po) - 1, *self._args(d_points, d_segments, po, so, out),
+                                          ctypes.c_void_p(st.ctypes.data), ctypes.c_void_p(stream))
+        return out, st, rc
+
+    def triangulate(self, instances):
+        """[(xy, cons), ...] host arrays -> [(tris, adj, cflags) or GcdtError] per instance."""
+        import torch
+        po, so = self.offsets(instances)
+        dev = torch.device("cuda", self.device)
+        xy = np.concatenate([np.asarray(x, np.int32).reshape(-1, 2) for x, _ in instances]) if po[-1] else np.zeros((0, 2), np.int32)
+        cs = [np.asarray(c, np.int32).reshape(-1, 2) for _, c in instances if c is not None and len(c)]
+        cons = np.concatenate(cs) if cs else np.zeros((0, 2), np.int32)
+        d_xy = torch.from_numpy(np.ascontiguousarray(xy)).to(dev)
+        d_c = torch.from_numpy(np.ascontiguousarray(cons)).to(dev) if len(cons) else None
+        out, st, rc = self.triangulate_device(d_xy, d_c, po, so)
+        tris, adj, cf = (o.cpu().numpy() for o in out)
+        res = []
+        for i in range(len(instances)):
+            if st[i] != 0:
+                res.append(GcdtError(int(st[i]), "instance %d" % i))
+                continue
+            t0 = int(2 * po[i] + 2 * i)
+            t1 = t0 + int(2 * (po[i + 1] - po[i]) + 2)
+            res.append((tris[t0:t1], adj[t0:t1], cf[t0:t1]))
+        return res
+
+    def autotune(self, d_points, d_segments, po, so, sample_instances=0, stream=None):
+        import torch
+        po = np.ascontiguousarray(po, np.int64)
+        so = np.ascontiguousarray(so, np.int64)
+        out = self.alloc_outputs(po)
+        cfg = BatchConfig()
+        if stream is None:
+            stream = torch.cuda.current_stream(torch.device("cuda", self.device)).cuda_stream
+        rc = lib().gcdt_batch_autotune(self._h, len(po) - 1, *self._args(d_points, d_segments, po, so, out),
+                                       int(sample_instances), ctypes.byref(cfg), ctypes.c_void_p(stream))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_batch_autotune")
+        return {"threads_per_instance": cfg.threads_per_instance, "sample_stride": cfg.sample_stride}
+
+    def set_config(self, threads_per_instance, sample_stride):
+        cfg = BatchConfig(threads_per_instance, sample_stride)
+        rc = lib().gcdt_batch_set_config(self._h, ctypes.byref(cfg))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_batch_set_config")
+
+    def get_config(self):
+        cfg = BatchConfig()
+        lib().gcdt_batch_get_config(self._h, ctypes.byref(cfg))
+        return {"threads_per_instance": cfg.threads_per_instance, "sample_stride": cfg.sample_stride}
+
+    def last_ms(self):
+        return float(lib().gcdt_batch_last_ms(self._h))

@@ -1,0 +1,181 @@
+// exec.cuh -- the two executors of the stage driver on the GPU.
+//
+//   GridExec   every block of a cooperative persistent launch: a phase is a
+//              grid-stride loop followed by a bounded grid barrier;
+//   BlockExec  one block: a phase is a block-stride loop followed by
+//              __syncthreads (the single-block tails of a solve, and every
+//              instance of the batched path).
+#pragma once
+#include "solver.cuh"
+
+namespace gcdt {
+
+// ---------------------------------------------------------------------------
+// Persistent stage kernel.  One cooperative launch runs every insertion
+// round, flip sub-round and constraint round of a solve; phases are
+// grid-stride loops separated by a grid barrier, so the round structure
+// costs no kernel launches and no host round trips.
+
+constexpr int kPersistBlock = 256;
+
+struct GridExec {
+    static constexpr bool kCanNarrow = true;
+    Counters* cnt;
+    unsigned nblocks;
+    __device__ int narrow_flips(Ctx& c, Driver& D, long long& nq);
+    __device__ int narrow_rounds(Ctx& c, Driver& D, long long nact);
+
+    // Snapshot of the head of Counters (status, error words, list cursors)
+    // taken by thread 0 right after each grid barrier: the driver's reads of
+    // these values come from shared memory instead of every thread reading
+    // the same L2 line.
+    static constexpr int kSnapWords = 12;   // 96 bytes: status..cur_scr
+    unsigned long long* snap;                // shared memory, kSnapWords entries
+
+    __device__ void take_snapshot() {
+        volatile unsigned long long* src = reinterpret_cast<volatile unsigned long long*>(cnt);
+        for (int k = 0; k < kSnapWords; ++k) snap[k] = src[k];
+    }
+
+    // Sense-free generation barrier.  Every wait is bounded: after ~2^24
+    // polls the block records ST_BARRIER and stops waiting, and once that bit
+    // is set no block waits or works any more, so the kernel always ends.
+    __device__ void barrier() {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            volatile unsigned* vgen = &cnt->bar_gen;
+            volatile int* vst = &cnt->status;
+            if (!(*vst & ST_BARRIER)) {
+                unsigned g = *vgen;
+                __threadfence();
+                unsigned arrived = atomicAdd(&cnt->bar_count, 1u);
+                if (arrived == nblocks - 1) {
+                    atomicExch(&cnt->bar_count, 0u);
+                    __threadfence();
+                    atomicAdd(&cnt->bar_gen, 1u);
+                } else {
+                    unsigned spins = 0;
+                    while (*vgen == g) {
+                        if (++spins > (1u << 24)) { atomicOr(&cnt->status, ST_BARRIER); break; }
+                        if (*vst & ST_BARRIER) break;
+                        __nanosleep(64);
+                    }
+                }
+            }
+            __threadfence();
+            take_snapshot();
+        }
+        __syncthreads();
+    }
+    __device__ void phase(int k, const Ctx& c, long long count) {
+        const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+        long long t0 = timer ? clock64() : 0;
+        if (!(word(&cnt->status) & ST_BARRIER)) {
+            long long stride = (long long)gridDim.x * blockDim.x;
+            for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+                dispatch(k, c, (int)i);
+        }
+        barrier();
+        if (timer && k < kMaxPhaseKinds) {   // phase time incl. the barrier, as block 0 sees it
+            cnt->phase_cyc[k] += clock64() - t0;
+            cnt->phase_cnt[k] += 1;
+        }
+    }
+    // Values read after a barrier come from the block's snapshot.
+    __device__ unsigned long long cursor(unsigned long long* p) {
+        size_t off = (size_t)((char*)p - (char*)cnt);
+        if (off + 8 <= kSnapWords * 8) return *reinterpret_cast<unsigned long long*>((char*)snap + off);
+        return *(volatile unsigned long long*)p;
+    }
+    __device__ int word(int* p) {
+        size_t off = (size_t)((char*)p - (char*)cnt);
+        if (off + 4 <= kSnapWords * 8) return *reinterpret_cast<int*>((char*)snap + off);
+        return *(volatile int*)p;
+    }
+    __device__ void finish(const Ctx&, long long rounds, long long subrounds, long long crounds, int rc) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            cnt->rounds = rounds;
+            cnt->flip_subrounds = subrounds;
+            cnt->constraint_rounds = crounds;
+            if (rc) atomicOr(&cnt->status, rc);
+        }
+    }
+};
+
+// Executor of one block: a phase is a block-stride loop and a block barrier.
+// Used by block 0 for the short tails while the other blocks wait.
+struct BlockExec {
+    static constexpr bool kCanNarrow = false;
+    Counters* cnt;
+    __device__ void phase(int k, const Ctx& c, long long count) {
+        for (long long i = threadIdx.x; i < count; i += blockDim.x) dispatch(k, c, (int)i);
+        __syncthreads();
+    }
+    __device__ unsigned long long cursor(unsigned long long* p) { return *(volatile unsigned long long*)p; }
+    __device__ int word(int* p) { return *(volatile int*)p; }
+    __device__ void finish(const Ctx&, long long rounds, long long subrounds, long long crounds, int rc) {
+        if (threadIdx.x == 0) {
+            cnt->rounds = rounds;
+            cnt->flip_subrounds = subrounds;
+            cnt->constraint_rounds = crounds;
+            if (rc) atomicOr(&cnt->status, rc);
+        }
+    }
+    __device__ int narrow_flips(Ctx&, Driver&, long long&) { return ST_INTERNAL; }
+    __device__ int narrow_rounds(Ctx&, Driver&, long long) { return ST_INTERNAL; }
+};
+
+static_assert(sizeof(Driver) <= sizeof(((Counters*)0)->handoff), "driver state fits the hand-off area");
+static_assert(sizeof(Driver) % 8 == 0, "driver state is whole 8-byte words");
+
+__device__ inline void store_handoff(Counters* cnt, const Driver& D, long long nq, int rc) {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&D);
+    for (unsigned k = 0; k < sizeof(Driver) / 8; ++k) cnt->handoff[k] = src[k];
+    cnt->handoff_nq = nq;
+    cnt->handoff_rc = rc;
+}
+
+__device__ inline int load_handoff(Counters* cnt, Driver& D, long long& nq) {
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&D);
+    volatile unsigned long long* src = cnt->handoff;
+    for (unsigned k = 0; k < sizeof(Driver) / 8; ++k) dst[k] = src[k];
+    nq = *(volatile long long*)&cnt->handoff_nq;
+    return *(volatile int*)&cnt->handoff_rc;
+}
+
+__device__ inline int GridExec::narrow_flips(Ctx& c, Driver& D, long long& nq) {
+    const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+    long long t0 = timer ? clock64() : 0;
+    if (blockIdx.x == 0) {
+        BlockExec bx{cnt};
+        Driver Db = D;
+        Ctx cb = c;
+        long long left = nq;
+        int rc = flip_loop(bx, cb, Db, left, 4 * kNarrowQueue);
+        if (threadIdx.x == 0) store_handoff(cnt, Db, left, rc);
+    }
+    barrier();
+    int rc = load_handoff(cnt, D, nq);
+    if (timer) { cnt->phase_cyc[K_NARROW_FLIPS] += clock64() - t0; cnt->phase_cnt[K_NARROW_FLIPS] += 1; }
+    return rc;
+}
+
+__device__ inline int GridExec::narrow_rounds(Ctx& c, Driver& D, long long nact) {
+    const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+    long long t0 = timer ? clock64() : 0;
+    if (blockIdx.x == 0) {
+        BlockExec bx{cnt};
+        Driver Db = D;
+        Ctx cb = c;
+        int rc = insert_rounds(bx, cb, Db, nact);
+        if (threadIdx.x == 0) store_handoff(cnt, Db, 0, rc);
+    }
+    barrier();
+    long long dummy;
+    int rc = load_handoff(cnt, D, dummy);
+    if (timer) { cnt->phase_cyc[K_NARROW_ROUNDS] += clock64() - t0; cnt->phase_cnt[K_NARROW_ROUNDS] += 1; }
+    return rc;
+}
+
+
+}  // namespace gcdt

@@ -13,7 +13,7 @@ struct Layout {
     size_t off[48];
     int count = 0;
     size_t total = 0;
-    size_t take(size_t bytes) {
+    __host__ __device__ size_t take(size_t bytes) {
         size_t o = total;
         total += (bytes + 255) & ~size_t(255);
         off[count++] = o;
@@ -31,7 +31,7 @@ struct Plan {
     size_t o_seg, o_pendA, o_pendB, o_pinfo, o_scratch, o_vt, o_lvl, o_cnt;
 };
 
-inline Plan make_plan(int64_t n, int64_t s, size_t sort_temp_bytes) {
+__host__ __device__ inline Plan make_plan(int64_t n, int64_t s, size_t sort_temp_bytes) {
     Plan p;
     p.n = n; p.s = s; p.ntri = 2 * n + 2;
     p.sort_temp_bytes = sort_temp_bytes;

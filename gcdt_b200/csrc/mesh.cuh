@@ -257,6 +257,17 @@ GCDT_HD void body_gather(const Ctx& c, int i) {
     }
 }
 
+// Per-solve reset of the per-triangle state, for solves whose arrays are
+// not cleared by the host (the batched path).
+GCDT_HD void body_clear(const Ctx& c, int t) {
+    c.vote[t] = 0;
+    c.claim[t] = 0;
+    c.ins[t] = make_int2(0, 0);
+    c.modR[t] = -1;
+    c.fst[t] = -1;
+    c.qst[t] = 0;
+}
+
 // Root triangles (rawMesh.cu:16-21) -- one thread.
 GCDT_HD void body_root(const Ctx& c, int) {
     int n = c.n;

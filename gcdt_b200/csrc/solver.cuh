@@ -24,6 +24,7 @@ enum Kern : int {
     K_FLIP_CHECK, K_FLIP_DO, K_FLIP_FIX, K_OUTPUT,
     K_SEG_INIT, K_CWALK, K_CCLAIM, K_CPROC,
     K_NARROW_FLIPS, K_NARROW_ROUNDS,     // timing labels of the single-block tails
+    K_CLEAR,
     K_COUNT
 };
 
@@ -36,7 +37,7 @@ struct SolveStats {
     long long host_syncs = 0;
 };
 
-inline Ctx bind_ctx(char* base, const Plan& p) {
+__host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     Ctx c{};
     c.n = (int)p.n; c.s = (int)p.s; c.ntri = (int)p.ntri;
     c.keys = (unsigned long long*)(base + p.o_keys);
@@ -102,6 +103,7 @@ GCDT_HD void dispatch(int k, const Ctx& c, int i) {
     case K_CWALK: body_cwalk(c, i); break;
     case K_CCLAIM: body_cclaim(c, i); break;
     case K_CPROC: body_cproc(c, i); break;
+    case K_CLEAR: body_clear(c, i); break;
     default: break;
     }
 }

@@ -102,6 +102,44 @@ const char* gcdt_phase_name(int32_t kind);
    inCircle used by the triangulator. */
 gcdt_status gcdt_eval_predicates(const int32_t* d_quads, int32_t n_cases, int32_t* d_out, void* stream);
 
+/* ---- Batched triangulation (no counterpart in the reference, which
+   triangulates one point set per process, kernel.cu:5332-5466).
+   Many independent instances in one launch: one segmented Morton sort,
+   then one block per instance running the full solve, largest first.
+   Instance i owns points [point_offsets[i], point_offsets[i+1]) of d_points
+   and segments [segment_offsets[i], segment_offsets[i+1]) of d_segments,
+   whose indices are local to the instance (0 .. n_i-1).  Its 2n_i+2
+   triangles are written at triangle 2*point_offsets[i] + 2*i of d_tris,
+   d_adj and d_cflags, with local vertex ids (corners n_i .. n_i+3) and local
+   adjacency: exactly the single solve's output for that instance.  The
+   offset arrays are host arrays of n_instances+1 entries starting at 0. */
+typedef struct gcdt_batch gcdt_batch;
+typedef struct {
+    int32_t threads_per_instance;   /* 128, 256 or 512 threads per instance block */
+    int32_t sample_stride;          /* first insertion level: every k-th point (16..256) */
+} gcdt_batch_config;
+
+gcdt_status gcdt_batch_create(gcdt_batch** batch, int device, int64_t max_instances,
+                              int64_t max_total_points, int64_t max_total_segments);
+void gcdt_batch_destroy(gcdt_batch* batch);
+gcdt_status gcdt_batch_triangulate(gcdt_batch* batch, int32_t n_instances,
+                                   const int64_t* point_offsets, const int64_t* segment_offsets,
+                                   const int32_t* d_points, const int32_t* d_segments,
+                                   int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                   int32_t* instance_status, void* stream);
+/* Times every configuration on the batch (or on sample_instances instances
+   spread over its size distribution), keeps the fastest for later calls
+   and reports it in *chosen. */
+gcdt_status gcdt_batch_autotune(gcdt_batch* batch, int32_t n_instances,
+                                const int64_t* point_offsets, const int64_t* segment_offsets,
+                                const int32_t* d_points, const int32_t* d_segments,
+                                int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                int32_t sample_instances, gcdt_batch_config* chosen, void* stream);
+gcdt_status gcdt_batch_set_config(gcdt_batch* batch, const gcdt_batch_config* cfg);
+gcdt_status gcdt_batch_get_config(const gcdt_batch* batch, gcdt_batch_config* cfg);
+/* CUDA-event time of the last gcdt_batch_triangulate call. */
+double gcdt_batch_last_ms(const gcdt_batch* batch);
+
 /* Allocation-free variant of gcdt_triangulate (no counterpart in the
    reference, whose stages all allocate from its MemCache pool).  For callers
    that cannot allocate device memory when they call in: plugins whose host
