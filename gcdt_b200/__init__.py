@@ -96,6 +96,24 @@ def lib():
     L.gcdt_batch_get_config.restype = ctypes.c_int
     L.gcdt_batch_last_ms.argtypes = [vp]
     L.gcdt_batch_last_ms.restype = ctypes.c_double
+    L.gcdt_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, vp]
+    L.gcdt_server_create.restype = ctypes.c_int
+    L.gcdt_server_destroy.argtypes = [vp]
+    L.gcdt_server_destroy.restype = None
+    L.gcdt_server_submit.argtypes = [vp, vp, i32, vp, i32, ctypes.POINTER(i64)]
+    L.gcdt_server_submit.restype = ctypes.c_int
+    L.gcdt_server_wait.argtypes = [vp, i64, i32, ctypes.POINTER(i32)]
+    L.gcdt_server_wait.restype = ctypes.c_int
+    L.gcdt_server_fetch.argtypes = [vp, i64, vp, vp, vp, ctypes.POINTER(i32)]
+    L.gcdt_server_fetch.restype = ctypes.c_int
+    L.gcdt_server_release.argtypes = [vp, i64]
+    L.gcdt_server_release.restype = ctypes.c_int
+    L.gcdt_server_request_times.argtypes = [vp, i64, vp, vp, vp]
+    L.gcdt_server_request_times.restype = ctypes.c_int
+    L.gcdt_server_get_stats.argtypes = [vp, vp]
+    L.gcdt_server_get_stats.restype = ctypes.c_int
+    L.gcdt_server_reset_stats.argtypes = [vp]
+    L.gcdt_server_reset_stats.restype = ctypes.c_int
     L.gcdt_eval_predicates.argtypes = [vp, i32, vp, vp]
     L.gcdt_eval_predicates.restype = ctypes.c_int
     _LIB = L
@@ -381,3 +399,94 @@ class BatchTriangulator:
 
     def last_ms(self):
         return float(lib().gcdt_batch_last_ms(self._h))
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("memory_budget_bytes", ctypes.c_int64), ("lanes", ctypes.c_int32),
+                ("max_batch_instances", ctypes.c_int32), ("max_batch_points", ctypes.c_int64),
+                ("max_batch_segments", ctypes.c_int64), ("lane_workspace_bytes", ctypes.c_int64),
+                ("big_request_points", ctypes.c_int64), ("max_request_points", ctypes.c_int64),
+                ("max_request_segments", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("batches", ctypes.c_int64), ("big_solves", ctypes.c_int64), ("queued", ctypes.c_int64),
+                ("resident_bytes", ctypes.c_int64), ("peak_resident_bytes", ctypes.c_int64),
+                ("fixed_bytes", ctypes.c_int64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("requests_per_s", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Server:
+    """Continuous-batching triangulation server (gcdt_server_* in include/gcdt.h)."""
+
+    def __init__(self, memory_budget_bytes=150 << 30, lanes=4, max_batch_instances=512,
+                 max_batch_points=4_000_000, max_batch_segments=200_000, big_request_points=400_000,
+                 max_request_points=1_100_000, max_request_segments=40_000, device=0):
+        cfg = ServerConfig(int(memory_budget_bytes), int(lanes), int(max_batch_instances), int(max_batch_points),
+                           int(max_batch_segments), 0, int(big_request_points), int(max_request_points),
+                           int(max_request_segments))
+        h = ctypes.c_void_p()
+        rc = lib().gcdt_server_create(ctypes.byref(h), int(device), ctypes.byref(cfg))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_server_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().gcdt_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, xy, cons=None):
+        xy = np.ascontiguousarray(xy, np.int32).reshape(-1, 2)
+        cons = np.ascontiguousarray(np.zeros((0, 2)) if cons is None else cons, np.int32).reshape(-1, 2)
+        rid = ctypes.c_int64()
+        rc = lib().gcdt_server_submit(self._h, ctypes.c_void_p(xy.ctypes.data), len(xy),
+                                      ctypes.c_void_p(cons.ctypes.data if len(cons) else 0), len(cons),
+                                      ctypes.byref(rid))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_server_submit")
+        return rid.value
+
+    def wait(self, rid, timeout_ms=-1):
+        done = ctypes.c_int32()
+        rc = lib().gcdt_server_wait(self._h, int(rid), int(timeout_ms), ctypes.byref(done))
+        return bool(done.value), rc
+
+    def fetch(self, rid, n):
+        T = 2 * n + 2
+        tris = np.empty((T, 3), np.int32)
+        adj = np.empty((T, 3), np.int32)
+        cf = np.empty(T, np.uint8)
+        nt = ctypes.c_int32()
+        rc = lib().gcdt_server_fetch(self._h, int(rid), ctypes.c_void_p(tris.ctypes.data),
+                                     ctypes.c_void_p(adj.ctypes.data), ctypes.c_void_p(cf.ctypes.data),
+                                     ctypes.byref(nt))
+        if rc != 0:
+            raise GcdtError(rc, "request %d" % rid)
+        return tris, adj, cf
+
+    def release(self, rid):
+        return lib().gcdt_server_release(self._h, int(rid))
+
+    def times(self, rid):
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        lib().gcdt_server_request_times(self._h, int(rid), ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+    def stats(self):
+        st = ServerStats()
+        lib().gcdt_server_get_stats(self._h, ctypes.byref(st))
+        return st.as_dict()
+
+    def reset_stats(self):
+        lib().gcdt_server_reset_stats(self._h)

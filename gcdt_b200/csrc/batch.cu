@@ -159,9 +159,38 @@ bool valid_cfg(const gcdt_batch_config& c) {
             c.sample_stride == 128 || c.sample_stride == 256);
 }
 
+}  // namespace
+
+// Launch half of a batched solve (asynchronous on `st`).  tri_off, when
+// given, places instance i's triangles at tri_off[i] instead of
+// 2*pt_off[i] + 2*i (the serving engine's resident output pool).
+gcdt_status gcdt_batch_launch(gcdt_batch* b, int32_t ninst, const int64_t* pt_off, const int64_t* seg_off,
+                              const int64_t* tri_off, const int32_t* d_points, const int32_t* d_segments,
+                              int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags, cudaStream_t st,
+                              const gcdt_batch_config& cfg);
+// Completion half: after `st` has finished, turn the instances' status bits
+// into codes; returns the first failure.
+gcdt_status gcdt_batch_finalize(gcdt_batch* b, int32_t ninst, int32_t* inst_status);
+
+namespace {
+
 gcdt_status run_batch(gcdt_batch* b, int32_t ninst, const int64_t* pt_off, const int64_t* seg_off,
                       const int32_t* d_points, const int32_t* d_segments, int32_t* d_tris, int32_t* d_adj,
                       uint8_t* d_cflags, int32_t* inst_status, cudaStream_t st, const gcdt_batch_config& cfg) {
+    if (ninst <= 0) return ninst == 0 ? GCDT_OK : GCDT_BAD_INPUT;
+    gcdt_status rc = gcdt_batch_launch(b, ninst, pt_off, seg_off, nullptr, d_points, d_segments, d_tris, d_adj,
+                                       d_cflags, st, cfg);
+    if (rc != GCDT_OK) return rc;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return GCDT_CUDA_ERROR;
+    return gcdt_batch_finalize(b, ninst, inst_status);
+}
+
+}  // namespace
+
+gcdt_status gcdt_batch_launch(gcdt_batch* b, int32_t ninst, const int64_t* pt_off, const int64_t* seg_off,
+                              const int64_t* tri_off, const int32_t* d_points, const int32_t* d_segments,
+                              int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags, cudaStream_t st,
+                              const gcdt_batch_config& cfg) {
     if (ninst <= 0) return ninst == 0 ? GCDT_OK : GCDT_BAD_INPUT;
     if (ninst > b->max_inst) return GCDT_OOM;
     int64_t total = pt_off[ninst] - pt_off[0], stotal = seg_off[ninst] - seg_off[0];
@@ -175,7 +204,7 @@ gcdt_status run_batch(gcdt_batch* b, int32_t ninst, const int64_t* pt_off, const
         d.pt_off = pt_off[i];
         d.seg_off = seg_off[i];
         d.ws_off = (long long)ws;
-        d.tri_off = 2 * pt_off[i] + 2 * (long long)i;
+        d.tri_off = tri_off ? tri_off[i] : 2 * pt_off[i] + 2 * (long long)i;
         d.n = (int)n;
         d.s = (int)s;
         d.status = 0;
@@ -223,7 +252,10 @@ gcdt_status run_batch(gcdt_batch* b, int32_t ninst, const int64_t* pt_off, const
     }
     if (cudaGetLastError() != cudaSuccess) return GCDT_CUDA_ERROR;
     cudaMemcpyAsync(b->h_desc, b->d_desc, sizeof(BatchDesc) * ninst, cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return GCDT_CUDA_ERROR;
+    return GCDT_OK;
+}
+
+gcdt_status gcdt_batch_finalize(gcdt_batch* b, int32_t ninst, int32_t* inst_status) {
     gcdt_status rc = GCDT_OK;
     for (int i = 0; i < ninst; ++i) {
         int bits = b->h_desc[i].status;
@@ -238,8 +270,6 @@ gcdt_status run_batch(gcdt_batch* b, int32_t ninst, const int64_t* pt_off, const
     }
     return rc;
 }
-
-}  // namespace
 
 extern "C" gcdt_status gcdt_batch_create(gcdt_batch** out, int device, int64_t max_instances,
                                          int64_t max_total_points, int64_t max_total_segments) {

@@ -140,6 +140,52 @@ gcdt_status gcdt_batch_get_config(const gcdt_batch* batch, gcdt_batch_config* cf
 /* CUDA-event time of the last gcdt_batch_triangulate call. */
 double gcdt_batch_last_ms(const gcdt_batch* batch);
 
+/* ---- Serving (no counterpart in the reference).  A scheduler thread
+   admits requests against a device-memory budget by their predicted
+   footprint (resident output (2n+2) x 25 bytes from the output pool, solve
+   workspace gcdt_workspace_bytes(n, s) from a lane), packs queued requests
+   into batches on `lanes` concurrent streams as lanes free up (continuous
+   batching: work of requests that arrive while others run overlaps theirs
+   on the device), runs requests of at least big_request_points points alone
+   on the whole GPU, and keeps every result resident until it is fetched or
+   released.  Submission copies the caller's host arrays; all calls are
+   thread-safe. */
+typedef struct gcdt_server gcdt_server;
+typedef struct {
+    int64_t memory_budget_bytes;    /* device bytes for arenas + resident outputs */
+    int32_t lanes;                  /* concurrent batch streams (1..16) */
+    int32_t max_batch_instances;    /* per lane batch */
+    int64_t max_batch_points;
+    int64_t max_batch_segments;
+    int64_t lane_workspace_bytes;   /* 0: gcdt_workspace_bytes(max_batch_points, max_batch_segments) */
+    int64_t big_request_points;     /* at least this many points: run alone on the whole GPU */
+    int64_t max_request_points;
+    int64_t max_request_segments;
+} gcdt_server_config;
+typedef struct {
+    int64_t submitted, completed, failed, batches, big_solves, queued;
+    int64_t resident_bytes, peak_resident_bytes, fixed_bytes;
+    double p50_ms, p99_ms, max_ms;   /* submission -> completion, host clock */
+    double requests_per_s;           /* completed / (last completion - first submission) */
+} gcdt_server_stats;
+
+gcdt_status gcdt_server_create(gcdt_server** server, int device, const gcdt_server_config* cfg);
+void gcdt_server_destroy(gcdt_server* server);
+gcdt_status gcdt_server_submit(gcdt_server* server, const int32_t* points, int32_t n,
+                               const int32_t* segments, int32_t s, int64_t* request_id);
+/* Wait up to timeout_ms (-1: no limit); *done tells whether it finished;
+   returns the request's status once done. */
+gcdt_status gcdt_server_wait(gcdt_server* server, int64_t request_id, int32_t timeout_ms, int32_t* done);
+/* Copy a finished result to host arrays sized for 2n+2 triangles, then
+   release it; blocks until the request is done. */
+gcdt_status gcdt_server_fetch(gcdt_server* server, int64_t request_id, int32_t* h_tris, int32_t* h_adj,
+                              uint8_t* h_cflags, int32_t* n_tris);
+gcdt_status gcdt_server_release(gcdt_server* server, int64_t request_id);
+gcdt_status gcdt_server_request_times(gcdt_server* server, int64_t request_id, double* submit_ms,
+                                      double* start_ms, double* done_ms);
+gcdt_status gcdt_server_get_stats(gcdt_server* server, gcdt_server_stats* out);
+gcdt_status gcdt_server_reset_stats(gcdt_server* server);
+
 /* Allocation-free variant of gcdt_triangulate (no counterpart in the
    reference, whose stages all allocate from its MemCache pool).  For callers
    that cannot allocate device memory when they call in: plugins whose host

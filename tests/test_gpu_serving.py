@@ -1,0 +1,72 @@
+"""Serving: every result is the same alone and in a concurrent mix, equal to
+the single solve; admission waits for memory instead of failing."""
+import threading
+
+import numpy as np
+import pytest
+
+import gcdt_b200 as g
+from tests.test_gpu_parity import canonical_with_flags
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(k, seed0, cap):
+    out = []
+    for i in range(k):
+        xy, cons = g.generate(g.GEN_SERVING_REQUEST, seed0 + i, 0)
+        if len(xy) > cap:
+            xy, cons = g.generate(g.GEN_SERVING_REQUEST, seed0 + i, cap)
+        out.append((xy, cons))
+    return out
+
+
+def test_same_alone_and_in_the_mix():
+    reqs = _requests(40, 700, cap=120_000)
+    probe = reqs[7]
+    sv = g.Server(memory_budget_bytes=24 << 30, lanes=3, max_batch_instances=64, max_batch_points=600_000,
+                  max_batch_segments=30_000, big_request_points=90_000, max_request_points=130_000,
+                  max_request_segments=10_000)
+    rid = sv.submit(*probe)
+    alone = sv.fetch(rid, len(probe[0]))
+    # the mix: three client threads submit concurrently, the probe among them
+    ids = [None] * len(reqs)
+
+    def client(part):
+        for i in part:
+            ids[i] = sv.submit(*reqs[i])
+
+    th = [threading.Thread(target=client, args=(range(k, len(reqs), 3),)) for k in range(3)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    results = [sv.fetch(ids[i], len(reqs[i][0])) for i in range(len(reqs))]
+    for a, b in zip(alone, results[7]):
+        assert np.array_equal(a, b)                      # byte for byte, alone vs in the mix
+    single = g.Triangulator(max(len(x) for x, _ in reqs), max(len(c) for _, c in reqs))
+    for (xy, cons), (t, a, c) in zip(reqs, results):
+        st, sa, sc = single.triangulate_host(xy, cons)
+        assert np.array_equal(canonical_with_flags(t, c), canonical_with_flags(st, sc))
+    st = sv.stats()
+    assert st["completed"] == len(reqs) + 1 and st["failed"] == 0
+    assert st["batches"] >= 1 and st["big_solves"] >= 1
+    single.close()
+    sv.close()
+
+
+def test_admission_waits_for_memory():
+    reqs = _requests(12, 900, cap=40_000)
+    # output pool sized for about three resident results at a time
+    fixed = (g.workspace_bytes(90_000, 4_000) + g.workspace_bytes(45_000, 2_000) +
+             8 * (90_000 + 4_000 + 45_000 + 2_000))
+    budget = fixed + 3 * (2 * 45_000 + 2) * 25 + (1 << 20)
+    sv = g.Server(memory_budget_bytes=budget, lanes=1, max_batch_instances=8, max_batch_points=90_000,
+                  max_batch_segments=4_000, big_request_points=1 << 30, max_request_points=45_000,
+                  max_request_segments=2_000)
+    ids = [sv.submit(*r) for r in reqs]
+    for i, rid in enumerate(ids):          # fetch in order; later requests get memory as earlier ones leave
+        t, a, c = sv.fetch(rid, len(reqs[i][0]))
+        assert len(t) == 2 * len(reqs[i][0]) + 2
+    assert sv.stats()["completed"] == len(reqs)
+    sv.close()
