@@ -386,8 +386,8 @@ def run_serving(args):
     rng = np.random.default_rng(2026)
     pool = [g.generate(g.GEN_SERVING_REQUEST, 1 + i) for i in range(args.pool)]
     sizes = np.array([len(x) for x, _ in pool])
-    sv = g.Server(memory_budget_bytes=150 << 30, lanes=4, max_batch_instances=512, max_batch_points=8_000_000,
-                  max_batch_segments=200_000, big_request_points=400_000,
+    sv = g.Server(memory_budget_bytes=150 << 30, lanes=4, max_batch_instances=512, max_batch_points=4_000_000,
+                  max_batch_segments=100_000, big_request_points=args.big_points,
                   max_request_points=int(sizes.max()) + 1, max_request_segments=int(max(len(c) for _, c in pool)) + 1)
     # warm-up
     for rid in [sv.submit(*pool[i]) for i in range(min(32, len(pool)))]:
@@ -438,7 +438,7 @@ def run_serving(args):
         "n_gpus": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "i64/i128 exact predicates on i32 coordinates (f64 filter)", "data": "synthetic",
         "config": {"workload": "serving: %d Poisson arrivals at 80%% of measured capacity, n log-uniform [1000, 1e6], coords [1, 2^28), ~2%% segments; requests drawn from %d distinct generated requests" % (nreq, len(pool)),
-                   "budget_bytes": 150 << 30, "lanes": 4, "big_request_points": 400_000,
+                   "budget_bytes": 150 << 30, "lanes": 4, "big_request_points": args.big_points,
                    "points_served": pts, "wall_s": wall},
         "server_stats": st,
     }
@@ -458,6 +458,8 @@ def main():
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--pool", type=int, default=256)
+    ap.add_argument("--big-points", type=int, default=30000,
+                    help="serving: requests with at least this many points use the whole-GPU solve")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-repeat", type=int, default=3)
     ap.add_argument("--validate", action="store_true")

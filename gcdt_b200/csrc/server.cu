@@ -12,9 +12,12 @@
 //     batch as soon as one of several lanes (each a stream with its own batch
 //     arena) is free, so requests that arrive while others run are launched
 //     next to them and their work overlaps on the device;
-//   - requests of at least big_request_points points run alone on the whole
-//     GPU through the single-solve path (cooperative launch), after the
-//     lanes drain;
+//   - requests of at least big_request_points points go to a second queue
+//     served by a worker thread that runs them one at a time on the whole GPU
+//     through the single-solve path, on a high-priority stream, concurrently
+//     with the lanes (the block scheduler favours the high-priority grid, and
+//     the single solve's bounded grid barrier turns any wait for blocks held
+//     by a lane into an error instead of a hang);
 //   - results stay resident in the output pool until the client fetches
 //     (copies out) or releases them.
 // Latency is measured on the host from submission to the moment the
@@ -124,10 +127,12 @@ struct gcdt_server {
     RangeAlloc alloc;
     std::mutex mu;
     std::condition_variable cv, done_cv;
-    std::deque<int64_t> queue;
+    std::deque<int64_t> queue;       // small requests, for the lanes
+    std::deque<int64_t> big_queue;   // large requests, for the big worker
     std::unordered_map<int64_t, Request> reqs;
     int64_t next_id = 1;
-    std::thread th;
+    std::thread th, big_th;
+    std::condition_variable big_cv;
     bool stop = false;
     gcdt_status fatal = GCDT_OK;
     std::chrono::steady_clock::time_point t0;
@@ -137,8 +142,9 @@ struct gcdt_server {
     size_t fixed_bytes = 0;
 
     void run();
+    void run_big_worker();
     bool dispatch_batch(std::unique_lock<std::mutex>& lk, Lane& L);
-    void run_big(std::unique_lock<std::mutex>& lk, int64_t id);
+    bool run_big(std::unique_lock<std::mutex>& lk, int64_t id);
     void complete(Request& r, gcdt_status st) {
         r.state = DONE;
         r.status = st;
@@ -163,7 +169,7 @@ struct DevGuard {
 };
 }  // namespace
 
-// Pack queued small requests (FIFO, stopping at a large one) into a batch on
+// Pack queued small requests (FIFO) into a batch on
 // lane L.  Called with the lock held; the lock is dropped while the inputs
 // are staged and the batch is launched.
 bool gcdt_server::dispatch_batch(std::unique_lock<std::mutex>& lk, Lane& L) {
@@ -175,7 +181,6 @@ bool gcdt_server::dispatch_batch(std::unique_lock<std::mutex>& lk, Lane& L) {
     const size_t ws_cap = (size_t)cfg.lane_workspace_bytes;
     while (!queue.empty() && (int)L.ids.size() < cfg.max_batch_instances) {
         Request& r = reqs[queue.front()];
-        if (r.n >= cfg.big_request_points) break;
         size_t need = gcdt_workspace_bytes(r.n, r.s);
         if (L.po.back() + r.n > cfg.max_batch_points || L.so.back() + r.s > cfg.max_batch_segments ||
             ws + need > ws_cap)
@@ -223,13 +228,14 @@ bool gcdt_server::dispatch_batch(std::unique_lock<std::mutex>& lk, Lane& L) {
     return true;
 }
 
-// A large request alone on the whole GPU (the lanes have drained).
-void gcdt_server::run_big(std::unique_lock<std::mutex>& lk, int64_t id) {
+// A large request on the whole GPU.  Returns false when the output pool
+// has no room yet.
+bool gcdt_server::run_big(std::unique_lock<std::mutex>& lk, int64_t id) {
     Request& r = reqs[id];
     int64_t ntri = 2 * (int64_t)r.n + 2;
     int64_t off = alloc.alloc(ntri);
-    if (off < 0) return;                    // wait for memory
-    queue.pop_front();
+    if (off < 0) return false;              // wait for memory
+    big_queue.pop_front();
     pool_used += ntri;
     pool_peak = std::max(pool_peak, pool_used);
     r.tri_off = off;
@@ -248,6 +254,17 @@ void gcdt_server::run_big(std::unique_lock<std::mutex>& lk, int64_t id) {
     lk.lock();
     complete(reqs[id], rc);
     done_cv.notify_all();
+    return true;
+}
+
+void gcdt_server::run_big_worker() {
+    DevGuard g(device);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        if (stop && big_queue.empty()) break;
+        if (big_queue.empty() || !run_big(lk, big_queue.front()))
+            big_cv.wait_for(lk, std::chrono::microseconds(100));
+    }
 }
 
 void gcdt_server::run() {
@@ -269,21 +286,10 @@ void gcdt_server::run() {
         }
         if (stop && queue.empty() && !any_busy) break;
         bool dispatched = false;
-        if (!queue.empty()) {
-            Request& head = reqs[queue.front()];
-            if (head.n >= cfg.big_request_points) {
-                if (!any_busy) {
-                    size_t q0 = queue.size();
-                    run_big(lk, head.id);
-                    dispatched = queue.size() != q0;
-                }
-            } else {
-                for (Lane& L : lanes) {
-                    if (L.busy || queue.empty()) continue;
-                    if (dispatch_batch(lk, L)) dispatched = true;
-                    else break;
-                }
-            }
+        for (Lane& L : lanes) {
+            if (L.busy || queue.empty()) continue;
+            if (dispatch_batch(lk, L)) dispatched = true;
+            else break;
         }
         if (!dispatched) cv.wait_for(lk, std::chrono::microseconds(50));
     }
@@ -306,6 +312,7 @@ extern "C" gcdt_status gcdt_server_create(gcdt_server** out, int device, const g
     DevGuard g(device);
     bool ok = true;
     size_t fixed = 0;
+    int lo_prio = 0, hi_prio = 0;
     sv->lanes.resize(c.lanes);
     for (Lane& L : sv->lanes) {
         ok = ok && gcdt_batch_create(&L.batch, device, c.max_batch_instances, c.max_batch_points,
@@ -319,7 +326,8 @@ extern "C" gcdt_status gcdt_server_create(gcdt_server** out, int device, const g
         fixed += (size_t)sv->cfg.lane_workspace_bytes + 8 * (size_t)(c.max_batch_points + c.max_batch_segments);
     }
     ok = ok && gcdt_create(&sv->big, device, c.max_request_points, c.max_request_segments) == GCDT_OK &&
-         cudaStreamCreateWithFlags(&sv->big_stream, cudaStreamNonBlocking) == cudaSuccess &&
+         cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio) == cudaSuccess &&
+         cudaStreamCreateWithPriority(&sv->big_stream, cudaStreamNonBlocking, hi_prio) == cudaSuccess &&
          cudaStreamCreateWithFlags(&sv->fetch_stream, cudaStreamNonBlocking) == cudaSuccess &&
          cudaMalloc(&sv->big_pts, 8 * (size_t)c.max_request_points) == cudaSuccess &&
          cudaMalloc(&sv->big_segs, 8 * (size_t)std::max<int64_t>(c.max_request_segments, 1)) == cudaSuccess;
@@ -343,20 +351,24 @@ extern "C" gcdt_status gcdt_server_create(gcdt_server** out, int device, const g
     }
     sv->t0 = std::chrono::steady_clock::now();
     sv->th = std::thread([sv] { sv->run(); });
+    sv->big_th = std::thread([sv] { sv->run_big_worker(); });
     *out = sv;
     return GCDT_OK;
 }
 
 extern "C" void gcdt_server_destroy(gcdt_server* sv) {
     if (!sv) return;
-    if (sv->th.joinable()) {
+    if (sv->th.joinable() || sv->big_th.joinable()) {
         {
             std::lock_guard<std::mutex> lk(sv->mu);
             sv->stop = true;
             sv->queue.clear();
+            sv->big_queue.clear();
         }
         sv->cv.notify_all();
-        sv->th.join();
+        sv->big_cv.notify_all();
+        if (sv->th.joinable()) sv->th.join();
+        if (sv->big_th.joinable()) sv->big_th.join();
     }
     DevGuard g(sv->device);
     for (Lane& L : sv->lanes) {
@@ -398,11 +410,13 @@ extern "C" gcdt_status gcdt_server_submit(gcdt_server* sv, const int32_t* points
         r.t_submit = now_ms(sv->t0);
         if (sv->first_submit < 0) sv->first_submit = r.t_submit;
         *request_id = r.id;
-        sv->queue.push_back(r.id);
+        if (r.n >= sv->cfg.big_request_points) sv->big_queue.push_back(r.id);
+        else sv->queue.push_back(r.id);
         sv->reqs.emplace(r.id, std::move(r));
         sv->submitted++;
     }
     sv->cv.notify_all();
+    sv->big_cv.notify_all();
     return GCDT_OK;
 }
 
@@ -429,6 +443,7 @@ static gcdt_status release_locked(gcdt_server* sv, int64_t id) {
     }
     sv->reqs.erase(it);
     sv->cv.notify_all();
+    sv->big_cv.notify_all();
     return GCDT_OK;
 }
 
@@ -491,7 +506,7 @@ extern "C" gcdt_status gcdt_server_get_stats(gcdt_server* sv, gcdt_server_stats*
     s.failed = sv->failed;
     s.batches = sv->batches;
     s.big_solves = sv->big_solves;
-    s.queued = (int64_t)sv->queue.size();
+    s.queued = (int64_t)(sv->queue.size() + sv->big_queue.size());
     s.resident_bytes = sv->pool_used * kTriBytes;
     s.peak_resident_bytes = sv->pool_peak * kTriBytes;
     s.fixed_bytes = (int64_t)sv->fixed_bytes;

@@ -146,9 +146,10 @@ double gcdt_batch_last_ms(const gcdt_batch* batch);
    workspace gcdt_workspace_bytes(n, s) from a lane), packs queued requests
    into batches on `lanes` concurrent streams as lanes free up (continuous
    batching: work of requests that arrive while others run overlaps theirs
-   on the device), runs requests of at least big_request_points points alone
-   on the whole GPU, and keeps every result resident until it is fetched or
-   released.  Submission copies the caller's host arrays; all calls are
+   on the device), runs requests of at least big_request_points points one at
+   a time on the whole GPU from a second worker on a high-priority stream,
+   concurrently with the lanes, and keeps every result resident until it is
+   fetched or released.  Submission copies the caller's host arrays; all calls are
    thread-safe. */
 typedef struct gcdt_server gcdt_server;
 typedef struct {
@@ -158,7 +159,7 @@ typedef struct {
     int64_t max_batch_points;
     int64_t max_batch_segments;
     int64_t lane_workspace_bytes;   /* 0: gcdt_workspace_bytes(max_batch_points, max_batch_segments) */
-    int64_t big_request_points;     /* at least this many points: run alone on the whole GPU */
+    int64_t big_request_points;     /* at least this many points: the whole-GPU single solve */
     int64_t max_request_points;
     int64_t max_request_segments;
 } gcdt_server_config;
