@@ -458,7 +458,7 @@ def main():
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--pool", type=int, default=256)
-    ap.add_argument("--big-points", type=int, default=30000,
+    ap.add_argument("--big-points", type=int, default=8000,
                     help="serving: requests with at least this many points use the whole-GPU solve")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-repeat", type=int, default=3)
