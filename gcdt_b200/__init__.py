@@ -114,6 +114,16 @@ def lib():
     L.gcdt_server_get_stats.restype = ctypes.c_int
     L.gcdt_server_reset_stats.argtypes = [vp]
     L.gcdt_server_reset_stats.restype = ctypes.c_int
+    L.gcdt_text_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+    L.gcdt_text_load.restype = vp
+    L.gcdt_text_sizes.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
+    L.gcdt_text_sizes.restype = None
+    L.gcdt_text_copy.argtypes = [vp, vp, vp]
+    L.gcdt_text_copy.restype = None
+    L.gcdt_text_free.argtypes = [vp]
+    L.gcdt_text_free.restype = None
+    L.gcdt_text_save.argtypes = [ctypes.c_char_p, vp, i64, vp, vp, vp, i64]
+    L.gcdt_text_save.restype = ctypes.c_int
     L.gcdt_eval_predicates.argtypes = [vp, i32, vp, vp]
     L.gcdt_eval_predicates.restype = ctypes.c_int
     _LIB = L
@@ -490,3 +500,33 @@ class Server:
 
     def reset_stats(self):
         lib().gcdt_server_reset_stats(self._h)
+
+
+def load_text(path):
+    """Read the reference's text input format -> (points (n,2) int32, segments (s,2) int32)."""
+    L = lib()
+    err = ctypes.c_int(0)
+    h = L.gcdt_text_load(os.fsencode(path), ctypes.byref(err))
+    if not h:
+        raise ValueError("cannot read %s (error %d)" % (path, err.value))
+    n = ctypes.c_int64()
+    s = ctypes.c_int64()
+    L.gcdt_text_sizes(h, ctypes.byref(n), ctypes.byref(s))
+    xy = np.zeros((n.value, 2), np.int32)
+    cons = np.zeros((s.value, 2), np.int32)
+    L.gcdt_text_copy(h, ctypes.c_void_p(xy.ctypes.data), ctypes.c_void_p(cons.ctypes.data))
+    L.gcdt_text_free(h)
+    return xy, cons
+
+
+def save_text(path, xy, tris, adj=None, cflags=None):
+    xy = np.ascontiguousarray(xy, np.int32)
+    tris = np.ascontiguousarray(tris, np.int32)
+    a = np.ascontiguousarray(adj, np.int32) if adj is not None else None
+    c = np.ascontiguousarray(cflags, np.uint8) if cflags is not None else None
+    rc = lib().gcdt_text_save(os.fsencode(path), ctypes.c_void_p(xy.ctypes.data), len(xy),
+                              ctypes.c_void_p(tris.ctypes.data),
+                              ctypes.c_void_p(a.ctypes.data if a is not None else 0),
+                              ctypes.c_void_p(c.ctypes.data if c is not None else 0), len(tris))
+    if rc != 0:
+        raise OSError("cannot write %s" % path)

@@ -187,6 +187,23 @@ gcdt_status gcdt_server_request_times(gcdt_server* server, int64_t request_id, d
 gcdt_status gcdt_server_get_stats(gcdt_server* server, gcdt_server_stats* out);
 gcdt_status gcdt_server_reset_stats(gcdt_server* server);
 
+/* ---- Input preprocessing and mesh export (host only).
+   gcdt_text_load reads the reference's text format (readFile,
+   kernel.cu:5159-5291): numPoints, "idx x y" lines, numCons, "idx a b"
+   lines; merges duplicate points, normalises the coordinates to the 2^30
+   grid as readFile + transPoints (kernel.cu:171-188) do, merges points that
+   collide on the grid, keeps them off the box, and drops degenerate and
+   repeated segments.  Returns a handle (NULL on error; *err = 1 cannot open,
+   2 malformed, 3 unknown point in a segment). */
+void* gcdt_text_load(const char* path, int* err);
+void gcdt_text_sizes(void* handle, int64_t* n_points, int64_t* n_segments);
+void gcdt_text_copy(void* handle, int32_t* points_xy, int32_t* segments);
+void gcdt_text_free(void* handle);
+/* Write a mesh as text: the n points and 4 corners, then one line per
+   triangle "idx a b c adj0 adj1 adj2 cflags".  Returns 0 on success. */
+int gcdt_text_save(const char* path, const int32_t* points_xy, int64_t n_points, const int32_t* tris,
+                   const int32_t* adj, const uint8_t* cflags, int64_t n_tris);
+
 /* Allocation-free variant of gcdt_triangulate (no counterpart in the
    reference, whose stages all allocate from its MemCache pool).  For callers
    that cannot allocate device memory when they call in: plugins whose host
