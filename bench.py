@@ -36,6 +36,11 @@ METRIC = "CDT Mpts/s at 10M pts+200k segs"
 UNIT = "Mpts/s"
 WORKLOAD = "plain CDT at scale: 10M Gaussian-mixture/uniform int32 points in [1,2^30-2]^2 + 3,125 star polygons (200,000 segments)"
 CPU_SAMPLE_POINTS = 2_000_000   # config-shaped sample for the CPU legs (18x18 polygon grid, 632 polygons)
+# DRAM bytes (read + write) of the stage kernel per point, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the same workload shape at
+# 1,020,608 points: 1,854,183,936 + 1,068,919,552 bytes.  Reported per solve as
+# this figure times N (the full-size capture would replay a 3 GB arena ~40x).
+DRAM_BYTES_PER_POINT = (1854183936 + 1068919552) / 1020608
 
 
 def rank_info():
@@ -261,7 +266,10 @@ def run_ours(args):
                        "parallelism": "replicas (one independent triangulation per GPU)" if world > 1 else "single GPU",
                        "l2": "256 MB buffer written between timed steps; working set ~2 GB"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": args.traffic,
+                         "frac": achieved / peak,
+                         "traffic": args.traffic if args.traffic is not None else DRAM_BYTES_PER_POINT * n,
+                         "traffic_source": "given" if args.traffic is not None else
+                                           "ncu DRAM bytes/point at 1.02M points x N",
                          "unit_of_work": "one full solve; algorithmic bytes 8N+8S+25(2N+2) = %d" % b_alg,
                          "peak_source": peak_kind},
             "cpu_baseline": cpu,
