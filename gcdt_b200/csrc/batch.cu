@@ -78,7 +78,9 @@ __global__ void __launch_bounds__(BS) gcdt_batch_solve(BatchArgs a) {
     c.out_tris = a.tris + 3 * d.tri_off;
     c.out_adj = a.adj + 3 * d.tri_off;
     c.out_cflags = a.cflags + d.tri_off;
-    c.stride[0] = a.stride0;
+    // small instances: two levels, the autotuned sample stride, then the rest
+    c.nlevels = 2;
+    c.stride[0] = a.stride0; c.stride[1] = 1;
     BlockExec ex{c.cnt};
     // per-solve reset: counters and the per-triangle state
     {

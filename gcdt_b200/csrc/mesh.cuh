@@ -114,7 +114,6 @@ struct Ctx {
     int* qst;                   // per triangle: queue stamp (dedup)
     int* queue;                 // flip queue (read)
     int* queue_next;            // flip queue (append)
-    int* flipped;               // flips of this sub-round (t of each pair)
 
     int4* seg;          // per segment: (a, b, stop, -)  sorted ids; a advances
     int* pend;          // pending segment list (read)
@@ -211,6 +210,28 @@ GCDT_HD int append_slot(unsigned long long* cur, unsigned long long base) {
     return (int)(b - base) + (int)g.thread_rank();
 #else
     unsigned long long o = *cur; *cur = o + 1; return (int)(o - base);
+#endif
+}
+
+// Append `cnt` consecutive elements (0 <= cnt <= 7); returns the index of
+// the first.  One atomic per warp; each thread's offset is the sum of the
+// counts of the lower lanes, taken bit by bit from three ballots.
+GCDT_HD int append_slots(unsigned long long* cur, unsigned long long base, int cnt) {
+#if defined(__CUDA_ARCH__)
+    const unsigned mask = __activemask();
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lt = mask & ((1u << lane) - 1u);
+    const unsigned b0 = __ballot_sync(mask, cnt & 1), b1 = __ballot_sync(mask, cnt & 2),
+                   b2 = __ballot_sync(mask, cnt & 4);
+    const unsigned before = __popc(b0 & lt) + 2u * __popc(b1 & lt) + 4u * __popc(b2 & lt);
+    const unsigned total = __popc(b0) + 2u * __popc(b1) + 4u * __popc(b2);
+    const int leader = __ffs(mask) - 1;
+    unsigned long long b = 0;
+    if ((int)lane == leader) b = atomicAdd(cur, (unsigned long long)total);
+    b = __shfl_sync(mask, b, leader);
+    return (int)(b - base) + (int)before;
+#else
+    unsigned long long o = *cur; *cur = o + (unsigned long long)cnt; return (int)(o - base);
 #endif
 }
 
@@ -353,7 +374,8 @@ GCDT_HD int locate_from_vertex(const Ctx& c, int a, int t, int2 p) {
 // Put the points of level c.level into the active list with their
 // triangle: the root triangles for level 0 (orient against the diagonal
 // (R,0)-(0,R), rawMesh.cu:37-57), otherwise a straight-line walk from the
-// Morton-preceding point of the previous level, which is already a vertex.
+// nearer of the previous level's Morton-preceding and Morton-following
+// points, which are already vertices.
 GCDT_HD void body_activate(const Ctx& c, int i) {
     if (c.lvl[i] != c.level) return;
     int t;
@@ -361,8 +383,19 @@ GCDT_HD void body_activate(const Ctx& c, int i) {
         int2 rd = make_int2(kBoxMax, 0), lt = make_int2(0, kBoxMax);
         t = orient2d(rd, lt, c.P[i]) >= 0 ? 0 : 1;
     } else {
-        int sv = i - i % c.stride[c.level - 1];
-        t = locate_from_vertex(c, sv, c.vt[sv], c.P[i]);
+        // start from the nearer of the two previous-level samples around i
+        // in Morton order (both are vertices already)
+        const int s = c.stride[c.level - 1];
+        int sv = i - i % s;
+        const int hi = sv + s;
+        const int2 p = c.P[i];
+        if (hi < c.n) {
+            int2 a = c.P[sv], b = c.P[hi];
+            long long da = (long long)(a.x - p.x) * (a.x - p.x) + (long long)(a.y - p.y) * (a.y - p.y);
+            long long db = (long long)(b.x - p.x) * (b.x - p.x) + (long long)(b.y - p.y) * (b.y - p.y);
+            if (db < da) sv = hi;
+        }
+        t = locate_from_vertex(c, sv, c.vt[sv], p);
         if (t < 0) { fail(c, ST_ITER_LIMIT); return; }
     }
     c.loc[i] = t;
@@ -529,9 +562,6 @@ GCDT_HD int qtri(int e) { return (int)((unsigned)e >> 3); }
 
 // The children of the inserted points are distinct triangles, so the first
 // flip queue of a round needs no de-duplication.
-GCDT_HD void push_queue(const Ctx& c, int t, int mask) {
-    c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = qentry(t, mask);
-}
 
 GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
     int4* row = &c.TA[ch];
@@ -561,7 +591,8 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
         resolve_split_edge(c, t, 0);
         resolve_split_edge(c, T1, 1);
         resolve_split_edge(c, T2, 2);
-        push_queue(c, t, 1); push_queue(c, T1, 2); push_queue(c, T2, 4);
+        int* qn = c.queue_next + append_slots(&c.cnt->cur_q, c.base_q, 3);
+        qn[0] = qentry(t, 1); qn[1] = qentry(T1, 2); qn[2] = qentry(T2, 4);
     } else {
         int e = code;
         int e1 = nx3(e), e_2 = nx3(e1);
@@ -573,8 +604,9 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
         resolve_split_edge(c, n, f1);
         resolve_split_edge(c, T2, f2);
         // outer edge and the half of the split edge
-        push_queue(c, t, (1 << e1) | (1 << e)); push_queue(c, T1, (1 << e_2) | (1 << e));
-        push_queue(c, n, (1 << f1) | (1 << e2)); push_queue(c, T2, (1 << f2) | (1 << e2));
+        int* qn = c.queue_next + append_slots(&c.cnt->cur_q, c.base_q, 4);
+        qn[0] = qentry(t, (1 << e1) | (1 << e)); qn[1] = qentry(T1, (1 << e_2) | (1 << e));
+        qn[2] = qentry(n, (1 << f1) | (1 << e2)); qn[3] = qentry(T2, (1 << f2) | (1 << e2));
     }
 }
 
@@ -637,11 +669,13 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     c.fst[n] = (int)c.sr;
     c.modR[t] = (int)c.round;
     c.modR[n] = (int)c.round;
-    c.flipped[append_slot(&c.cnt->cur_flip, c.base_flip)] = t;
-    // the new diagonal AD is locally Delaunay: queue the four outer edges
-    int qi = append_slot(&c.cnt->cur_q, c.base_q);
-    c.queue_next[qi] = qentry(t, 5);    // (A,B,D): BD and AB
-    c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = qentry(n, 3);   // (A,D,C): DC and CA
+    // The new diagonal AD is locally Delaunay: queue the four outer edges.
+    // Flip number f of the sub-round owns entries 2f, 2f+1 of the next
+    // queue; body_flip_fix reads the pairs from there and appends the
+    // re-queued losers after them.
+    int* qn = c.queue_next + 2 * append_slot(&c.cnt->cur_flip, c.base_flip);
+    qn[0] = qentry(t, 5);    // (A,B,D): BD and AB
+    qn[1] = qentry(n, 3);    // (A,D,C): DC and CA
 }
 
 GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
@@ -658,15 +692,16 @@ GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
 
 // k < c.list_n: resolve the outer adjacency of flipped pair k.
 // Otherwise queue entry k - c.list_n: a candidate that did not flip and
-// whose triangle nobody flipped goes back to the queue.
+// whose triangle nobody flipped goes back to the queue, after the
+// 2 * c.list_n entries of the flipped pairs.
 GCDT_HD void body_flip_fix(const Ctx& c, int k) {
     if (k >= c.list_n) {
         int2 cd = c.cand[k - c.list_n];
         if (cd.x >= 0 && c.fst[cd.x >> 2] != (int)c.sr)
-            c.queue_next[append_slot(&c.cnt->cur_q, c.base_q)] = c.queue[k - c.list_n];
+            c.queue_next[2 * c.list_n + append_slot(&c.cnt->cur_q, c.base_q)] = c.queue[k - c.list_n];
         return;
     }
-    int t = c.flipped[k];
+    int t = qtri(c.queue_next[2 * k]);
     int n = c.TA[t].y >> 2;
     resolve_flip_edge(c, t, 0);
     resolve_flip_edge(c, t, 2);

@@ -64,7 +64,6 @@ __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     c.qst = (int*)(base + p.o_qst);
     c.queue = (int*)(base + p.o_qA);
     c.queue_next = (int*)(base + p.o_qB);
-    c.flipped = (int*)(base + p.o_flipped);
     c.seg = (int4*)(base + p.o_seg);
     c.pend = (int*)(base + p.o_pendA);
     c.pend_next = (int*)(base + p.o_pendB);
@@ -74,10 +73,10 @@ __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     c.vt = (int*)(base + p.o_vt);
     c.lvl = (unsigned char*)(base + p.o_lvl);
     c.cnt = (Counters*)(base + p.o_cnt);
-    // two levels: every 64th point of the Morton order plus all segment
-    // endpoints, then the rest
-    c.nlevels = 2;
-    c.stride[0] = 64; c.stride[1] = 1; c.stride[2] = 1; c.stride[3] = 1;
+    // three levels: every 512th point of the Morton order plus all segment
+    // endpoints, then every 32nd, then the rest
+    c.nlevels = 3;
+    c.stride[0] = 512; c.stride[1] = 32; c.stride[2] = 1; c.stride[3] = 1;
     return c;
 }
 
@@ -170,11 +169,13 @@ GCDT_HD int flip_loop(EX& ex, Ctx& c, Driver& D, long long& nq, long long max_nq
         if (D.errs) return D.errs;
         long long nflip = (long long)(D.e_flip - c.base_flip);
         c.list_n = (int)nflip;
-        run_phase(ex, c, D, K_FLIP_FIX, nflip + nq);   // FLIP_DO and FLIP_FIX both append the next queue
+        // next queue: the flipped pairs' 2 * nflip entries, then the losers
+        // FLIP_FIX appends through cur_q
+        run_phase(ex, c, D, K_FLIP_FIX, nflip + nq);
         D.e_q = ex.cursor(&c.cnt->cur_q);
         D.subrounds++;
         D.sr++;
-        nq = (long long)(D.e_q - c.base_q);
+        nq = 2 * nflip + (long long)(D.e_q - c.base_q);
         int* t = D.qa; D.qa = D.qb; D.qb = t;
     }
     return 0;
