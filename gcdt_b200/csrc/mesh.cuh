@@ -5,10 +5,12 @@
 // Layout in HBM (structure of arrays, one row per point or triangle):
 //   P[v]      int2   point v in Morton-sorted order; corners at N..N+3
 //   perm[v]   int    input index of sorted point v (corners map to N+k)
-//   TV[t]     int4   (v0, v1, v2, cflags) -- CCW vertices, bit k of .w set when
-//                    the edge opposite v_k is a constraint edge
-//   TA[t]     int4   (a0, a1, a2, -)  a_k = 4*n + j: neighbour n across the
+//   tri[2t]   int4   TV: (v0, v1, v2, cflags) -- CCW vertices, bit k of .w set
+//                    when the edge opposite v_k is a constraint edge
+//   tri[2t+1] int4   TA: (a0, a1, a2, -)  a_k = 4*n + j: neighbour n across the
 //                    edge opposite v_k, which is opposite slot j in n; -1 = box
+//                    (TV and TA of a triangle share one 32-byte sector: most
+//                    visits read both)
 // Triangle slots never move: the two root triangles are 0 and 1, and sorted
 // point q creates exactly two new slots, 2+2q and 3+2q, when it is inserted
 // (1->3 split of one triangle, or 2->4 split of the two triangles sharing the
@@ -95,8 +97,7 @@ struct Ctx {
     int* perm;
     int* rank;
 
-    int4* TV;
-    int4* TA;
+    int4* tri;      // per triangle: vertices (TV) then adjacency (TA), 32 bytes
 
     int* loc;                 // triangle holding an uninserted point, -1 once inserted
     signed char* pedge;       // slot of the edge the point lies on, -1 inside
@@ -149,6 +150,10 @@ GCDT_HD void setc(int4& v, int i, int x) {
     if (i == 0) v.x = x; else if (i == 1) v.y = x; else v.z = x;
 }
 GCDT_HD int slot_of(const int4& tv, int v) { return tv.x == v ? 0 : (tv.y == v ? 1 : 2); }
+
+// Vertex row (TV) and adjacency row (TA) of triangle t.
+GCDT_HD int4& tri_v(const Ctx& c, int t) { return c.tri[2 * (size_t)(unsigned)t]; }
+GCDT_HD int4& tri_a(const Ctx& c, int t) { return c.tri[2 * (size_t)(unsigned)t + 1]; }
 
 GCDT_HD uint32_t hash32(uint32_t x) {  // bijective 32-bit mix
     x ^= x >> 16; x *= 0x7feb352dU;
@@ -292,10 +297,10 @@ GCDT_HD void body_clear(const Ctx& c, int t) {
 // Root triangles (rawMesh.cu:16-21) -- one thread.
 GCDT_HD void body_root(const Ctx& c, int) {
     int n = c.n;
-    c.TV[0] = make_int4(n, n + 1, n + 3, 0);
-    c.TV[1] = make_int4(n + 1, n + 2, n + 3, 0);
-    c.TA[0] = make_int4(enc(1, 1), -1, -1, 0);
-    c.TA[1] = make_int4(-1, enc(0, 0), -1, 0);
+    tri_v(c, 0) = make_int4(n, n + 1, n + 3, 0);
+    tri_v(c, 1) = make_int4(n + 1, n + 2, n + 3, 0);
+    tri_a(c, 0) = make_int4(enc(1, 1), -1, -1, 0);
+    tri_a(c, 1) = make_int4(-1, enc(0, 0), -1, 0);
 }
 
 // Level of each sorted point: a Morton-stratified sample first (every
@@ -326,7 +331,7 @@ GCDT_HD int locate_from_vertex(const Ctx& c, int a, int t, int2 p) {
         int2 pa = c.P[a];
         int t0 = t, found = -1, fslot = 0, u = -1, w = -1;
         for (int g = 0; g < 4096; ++g) {
-            int4 tv = c.TV[t];
+            int4 tv = tri_v(c, t);
             int i = slot_of(tv, a), i1 = nx3(i), i2 = nx3(i1);
             u = comp(tv, i1); w = comp(tv, i2);
             int2 pu = c.P[u], pw = c.P[w];
@@ -343,7 +348,7 @@ GCDT_HD int locate_from_vertex(const Ctx& c, int a, int t, int2 p) {
                 if (orient2d(pu, pw, p) >= 0) return t;
                 found = t; fslot = i; break;
             }
-            int nb = comp(c.TA[t], i2);
+            int nb = comp(tri_a(c, t), i2);
             if (nb < 0) return -1;
             t = nb >> 2;
             if (t == t0) return -1;
@@ -353,10 +358,10 @@ GCDT_HD int locate_from_vertex(const Ctx& c, int a, int t, int2 p) {
         int cur = found, cs = fslot;
         int next_a = -1;
         for (int steps = 0; steps < (1 << 22); ++steps) {
-            int en = comp(c.TA[cur], cs);
+            int en = comp(tri_a(c, cur), cs);
             if (en < 0) return -1;
             int n = en >> 2, j = en & 3;
-            int x = comp(c.TV[n], j);
+            int x = comp(tri_v(c, n), j);
             int2 px = c.P[x];
             // n = (x, w, u): p is inside iff it is left of (u,x) and (x,w)
             if (orient2d(c.P[u], px, p) >= 0 && orient2d(px, c.P[w], p) >= 0) return n;
@@ -420,7 +425,7 @@ GCDT_HD void body_vt_live(const Ctx& c, int k) {
     if (k >= 2 && c.lvl[k - 2] >= c.level) return;
     int t0 = k < 2 ? k : 2 * k - 2, nt = k < 2 ? 1 : 2;
     for (int t = t0; t < t0 + nt; ++t) {
-        int4 tv = c.TV[t];
+        int4 tv = tri_v(c, t);
         at_min(&c.vt[tv.x], t); at_min(&c.vt[tv.y], t); at_min(&c.vt[tv.z], t);
     }
 }
@@ -431,7 +436,7 @@ GCDT_HD void body_vt_live(const Ctx& c, int k) {
 // Terminates in a Delaunay triangulation (acyclic in-front-of relation).
 GCDT_HD int walk(const Ctx& c, int t, int2 p, int limit, int* steps) {
     for (int it = 0; it < limit; ++it) {
-        int4 tv = c.TV[t];
+        int4 tv = tri_v(c, t);
         int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
         int side = -1;
         int r = it % 3;
@@ -441,7 +446,7 @@ GCDT_HD int walk(const Ctx& c, int t, int2 p, int limit, int* steps) {
             if (o < 0) side = s;
         }
         if (side < 0) { *steps += it; return t; }
-        int nb = comp(c.TA[t], side);
+        int nb = comp(tri_a(c, t), side);
         if (nb < 0) { *steps += it; return -1; }
         t = nb >> 2;
     }
@@ -461,13 +466,13 @@ GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
     if (c.modR[t] == (int)c.round - 1) {
         int steps = 0;
         int nt = walk(c, t, p, 256, &steps);
-        if (nt < 0) nt = locate_from_vertex(c, c.TV[t].x, t, p);
+        if (nt < 0) nt = locate_from_vertex(c, tri_v(c, t).x, t, p);
         if (nt < 0) { fail(c, ST_ITER_LIMIT); return; }
         t = nt;
         c.loc[q] = t;
     }
     c.act_next[append_slot(&c.cnt->cur_act, c.base_act)] = q;
-    int4 tv = c.TV[t];
+    int4 tv = tri_v(c, t);
     int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
     int o0 = orient2d(b, cc, p), o1 = orient2d(cc, a, p), o2 = orient2d(a, b, p);
     int e = o0 == 0 ? 0 : (o1 == 0 ? 1 : (o2 == 0 ? 2 : -1));
@@ -476,7 +481,7 @@ GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
     unsigned long long key = ((unsigned long long)c.round << 32) | (0xffffffffu - hash32((uint32_t)q));
     if (c.vote[t] < key) at_max64(&c.vote[t], key);
     if (e >= 0) {
-        int n = comp(c.TA[t], e) >> 2;
+        int n = comp(tri_a(c, t), e) >> 2;
         if (c.vote[n] < key) at_max64(&c.vote[n], key);
     }
 }
@@ -491,7 +496,7 @@ GCDT_HD void body_split(const Ctx& c, int k) {
     if (c.vote[t] != key) return;
     int e = c.pedge[q];
     int T1 = 2 + 2 * q, T2 = 3 + 2 * q;
-    int4 tv = c.TV[t], ta = c.TA[t];
+    int4 tv = tri_v(c, t), ta = tri_a(c, t);
     int fl = tv.w;
     if (e < 0) {
         int ch[3] = {t, T1, T2};
@@ -501,8 +506,8 @@ GCDT_HD void body_split(const Ctx& c, int k) {
             a.w = 0;
             for (int kk = 0; kk < 3; ++kk)
                 setc(a, kk, kk == j ? comp(ta, j) : enc(ch[kk], j));
-            c.TV[ch[j]] = v;
-            c.TA[ch[j]] = a;
+            tri_v(c, ch[j]) = v;
+            tri_a(c, ch[j]) = a;
         }
         c.ins[t] = make_int2((int)c.round, q * 8 + 7);
         c.modR[t] = (int)c.round;
@@ -510,7 +515,7 @@ GCDT_HD void body_split(const Ctx& c, int k) {
         int en = comp(ta, e);
         int n = en >> 2, e2 = en & 3;
         if (c.vote[n] != key) return;
-        int4 nv = c.TV[n], na = c.TA[n];
+        int4 nv = tri_v(c, n), na = tri_a(c, n);
         int gl = nv.w;
         // children: A1 = child_{e+1}(t) -> t, A2 = child_{e+2}(t) -> T1,
         //           B1 = child_{e2+1}(n) -> n, B2 = child_{e2+2}(n) -> T2
@@ -521,22 +526,22 @@ GCDT_HD void body_split(const Ctx& c, int k) {
         v = tv; setc(v, e1, q); v.w = fl & ((1 << e1) | (1 << e));
         a = make_int4(0, 0, 0, 0);
         setc(a, e1, comp(ta, e1)); setc(a, e_2, enc(A2, e1)); setc(a, e, enc(B2, e2));
-        c.TV[A1] = v; c.TA[A1] = a;
+        tri_v(c, A1) = v; tri_a(c, A1) = a;
         // A2
         v = tv; setc(v, e_2, q); v.w = fl & ((1 << e_2) | (1 << e));
         a = make_int4(0, 0, 0, 0);
         setc(a, e_2, comp(ta, e_2)); setc(a, e1, enc(A1, e_2)); setc(a, e, enc(B1, e2));
-        c.TV[A2] = v; c.TA[A2] = a;
+        tri_v(c, A2) = v; tri_a(c, A2) = a;
         // B1
         v = nv; setc(v, f1, q); v.w = gl & ((1 << f1) | (1 << e2));
         a = make_int4(0, 0, 0, 0);
         setc(a, f1, comp(na, f1)); setc(a, f2, enc(B2, f1)); setc(a, e2, enc(A2, e));
-        c.TV[B1] = v; c.TA[B1] = a;
+        tri_v(c, B1) = v; tri_a(c, B1) = a;
         // B2
         v = nv; setc(v, f2, q); v.w = gl & ((1 << f2) | (1 << e2));
         a = make_int4(0, 0, 0, 0);
         setc(a, f2, comp(na, f2)); setc(a, f1, enc(B1, f2)); setc(a, e2, enc(A1, e));
-        c.TV[B2] = v; c.TA[B2] = a;
+        tri_v(c, B2) = v; tri_a(c, B2) = a;
         c.ins[t] = make_int2((int)c.round, q * 8 + e);
         c.ins[n] = make_int2((int)c.round, q * 8 + 3 + e2);
         c.modR[t] = (int)c.round;
@@ -564,7 +569,7 @@ GCDT_HD int qtri(int e) { return (int)((unsigned)e >> 3); }
 // flip queue of a round needs no de-duplication.
 
 GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
-    int4* row = &c.TA[ch];
+    int4* row = &tri_a(c, ch);
     int old = comp(*row, s);
     if (old < 0) return;
     int m = old >> 2, ms = old & 3;
@@ -572,7 +577,7 @@ GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
     if (im.x == (int)c.round) {
         ((int*)row)[s] = enc(split_child(im, m, ms), ms);
     } else {
-        ((int*)&c.TA[m])[ms] = enc(ch, s);
+        ((int*)&tri_a(c, m))[ms] = enc(ch, s);
     }
 }
 
@@ -596,7 +601,7 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
     } else {
         int e = code;
         int e1 = nx3(e), e_2 = nx3(e1);
-        int en = comp(c.TA[T1], e);     // A2 slot e = enc(B1, e2)
+        int en = comp(tri_a(c, T1), e);     // A2 slot e = enc(B1, e2)
         int n = en >> 2, e2 = en & 3;
         int f1 = nx3(e2), f2 = nx3(f1);
         resolve_split_edge(c, t, e1);
@@ -620,14 +625,14 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
 GCDT_HD void body_flip_check(const Ctx& c, int k) {
     int qe = c.queue[k];
     int t = qtri(qe), mask = qe & 7;
-    int4 tv = c.TV[t], ta = c.TA[t];
+    int4 tv = tri_v(c, t), ta = tri_a(c, t);
     int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
     for (int i = 0; i < 3; ++i) {
         if (!((mask >> i) & 1)) continue;
         int en = comp(ta, i);
         if (en < 0 || ((tv.w >> i) & 1)) continue;
         int n = en >> 2, j = en & 3;
-        int d = comp(c.TV[n], j);
+        int d = comp(tri_v(c, n), j);
         if (incircle_sos(a, b, cc, c.P[d]) > 0) {
             int key = enc(t, i);
             unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)key));
@@ -652,14 +657,14 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     int n = cd.y >> 2, j = cd.y & 3;
     unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)cd.x));
     if (c.claim[t] != ck || c.claim[n] != ck) return;
-    int4 tv = c.TV[t], ta = c.TA[t], nv = c.TV[n], na = c.TA[n];
+    int4 tv = tri_v(c, t), ta = tri_a(c, t), nv = tri_v(c, n), na = tri_a(c, n);
     int i1 = nx3(i), i2 = nx3(i1), j1 = nx3(j), j2 = nx3(j1);
     int A = comp(tv, i), B = comp(tv, i1), C = comp(tv, i2), D = comp(nv, j);
     int ft = tv.w, fn = nv.w;
-    c.TV[t] = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
-    c.TA[t] = make_int4(comp(na, j1), enc(n, 2), comp(ta, i2), 0);
-    c.TV[n] = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
-    c.TA[n] = make_int4(comp(na, j2), comp(ta, i1), enc(t, 1), 0);
+    tri_v(c, t) = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
+    tri_a(c, t) = make_int4(comp(na, j1), enc(n, 2), comp(ta, i2), 0);
+    tri_v(c, n) = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
+    tri_a(c, n) = make_int4(comp(na, j2), comp(ta, i1), enc(t, 1), 0);
     int4 mt = make_int4(-1, -1, -1, 0), mn = make_int4(-1, -1, -1, 0);
     setc(mt, i1, enc(n, 1)); setc(mt, i2, enc(t, 2));
     setc(mn, j1, enc(t, 0)); setc(mn, j2, enc(n, 0));
@@ -679,14 +684,14 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
 }
 
 GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
-    int4* row = &c.TA[tt];
+    int4* row = &tri_a(c, tt);
     int old = comp(*row, s);
     if (old < 0) return;
     int m = old >> 2, ms = old & 3;
     if (c.fst[m] == (int)c.sr) {
         ((int*)row)[s] = comp(c.fmap[m], ms);
     } else {
-        ((int*)&c.TA[m])[ms] = enc(tt, s);
+        ((int*)&tri_a(c, m))[ms] = enc(tt, s);
     }
 }
 
@@ -702,7 +707,7 @@ GCDT_HD void body_flip_fix(const Ctx& c, int k) {
         return;
     }
     int t = qtri(c.queue_next[2 * k]);
-    int n = c.TA[t].y >> 2;
+    int n = tri_a(c, t).y >> 2;
     resolve_flip_edge(c, t, 0);
     resolve_flip_edge(c, t, 2);
     resolve_flip_edge(c, n, 0);
@@ -724,9 +729,9 @@ GCDT_HD void body_seg_init(const Ctx& c, int k) {
 }
 
 GCDT_HD void mark_edge(const Ctx& c, int t, int s) {
-    at_or(&c.TV[t].w, 1 << s);
-    int en = comp(c.TA[t], s);
-    if (en >= 0) at_or(&c.TV[en >> 2].w, 1 << (en & 3));
+    at_or(&tri_v(c, t).w, 1 << s);
+    int en = comp(tri_a(c, t), s);
+    if (en >= 0) at_or(&tri_v(c, en >> 2).w, 1 << (en & 3));
 }
 
 // Walk from the current start vertex a of a pending segment towards b.
@@ -749,7 +754,7 @@ GCDT_HD void body_cwalk(const Ctx& c, int k) {
         int t0 = c.vt[a], t = t0;
         int found = -1, fslot = 0, via = -1, et = -1, es = 0;
         for (int g2 = 0; g2 < (1 << 16); ++g2) {
-            int4 tv = c.TV[t];
+            int4 tv = tri_v(c, t);
             int i = slot_of(tv, a), i1 = nx3(i), i2 = nx3(i1);
             int u = comp(tv, i1), w = comp(tv, i2);
             if (u == b) { via = b; et = t; es = i2; break; }
@@ -759,7 +764,7 @@ GCDT_HD void body_cwalk(const Ctx& c, int k) {
             if (ou == 0 && dot3(pa, pu, pb) > 0) { via = u; et = t; es = i2; break; }
             if (ow == 0 && dot3(pa, pw, pb) > 0) { via = w; et = t; es = i1; break; }
             if (ou > 0 && ow < 0) { found = t; fslot = i; break; }
-            int nb = comp(c.TA[t], i2);
+            int nb = comp(tri_a(c, t), i2);
             if (nb < 0) break;
             t = nb >> 2;
             if (t == t0) break;
@@ -772,12 +777,12 @@ GCDT_HD void body_cwalk(const Ctx& c, int k) {
         if (found < 0) { fail(c, ST_CONSTRAINT_FAIL); c.pinfo[k] = make_int4(-1, 0, 0, 0); return; }
         int cur = found, cs = fslot, count = 1, stop = -1;
         for (int steps = 0; steps <= c.ntri; ++steps) {
-            int4 tv = c.TV[cur];
+            int4 tv = tri_v(c, cur);
             if ((tv.w >> cs) & 1) { fail(c, ST_CONSTRAINT_FAIL); c.pinfo[k] = make_int4(-1, 0, 0, 0); return; }
-            int en = comp(c.TA[cur], cs);
+            int en = comp(tri_a(c, cur), cs);
             if (en < 0) { fail(c, ST_CONSTRAINT_FAIL); c.pinfo[k] = make_int4(-1, 0, 0, 0); return; }
             int n = en >> 2, j = en & 3;
-            int x = comp(c.TV[n], j);
+            int x = comp(tri_v(c, n), j);
             count++;
             if (x == b) { stop = b; break; }
             int ox = orient2d(pa, pb, c.P[x]);
@@ -815,18 +820,18 @@ GCDT_HD void body_cclaim(const Ctx& c, int k) {
     int cur = pi.x >> 2, cs = pi.x & 3;
     L[0] = cur;
     for (int m = 1; m < kt; ++m) {
-        int en = comp(c.TA[cur], cs);
+        int en = comp(tri_a(c, cur), cs);
         int n = en >> 2, j = en & 3;
         L[m] = n;
         if (m == kt - 1) break;
-        int x = comp(c.TV[n], j);
+        int x = comp(tri_v(c, n), j);
         int ox = orient2d(pa, pb, c.P[x]);
         cur = n;
         cs = ox < 0 ? nx3(nx3(j)) : nx3(j);
     }
     int nr = 0;
     for (int m = 0; m < kt; ++m) {
-        int4 ta = c.TA[L[m]];
+        int4 ta = tri_a(c, L[m]);
         for (int s = 0; s < 3; ++s) {
             int en = comp(ta, s);
             if (en < 0) continue;
@@ -843,22 +848,22 @@ GCDT_HD void body_cclaim(const Ctx& c, int k) {
 // Flip the edge opposite slot i of t and update every neighbour in place
 // (the caller owns t, its partner and their neighbours).
 GCDT_HD int flip_local(const Ctx& c, int t, int i) {
-    int4 tv = c.TV[t], ta = c.TA[t];
+    int4 tv = tri_v(c, t), ta = tri_a(c, t);
     int en = comp(ta, i);
     int n = en >> 2, j = en & 3;
-    int4 nv = c.TV[n], na = c.TA[n];
+    int4 nv = tri_v(c, n), na = tri_a(c, n);
     int i1 = nx3(i), i2 = nx3(i1), j1 = nx3(j), j2 = nx3(j1);
     int A = comp(tv, i), B = comp(tv, i1), C = comp(tv, i2), D = comp(nv, j);
     int ft = tv.w, fn = nv.w;
     int oBD = comp(na, j1), oAB = comp(ta, i2), oDC = comp(na, j2), oCA = comp(ta, i1);
-    c.TV[t] = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
-    c.TA[t] = make_int4(oBD, enc(n, 2), oAB, 0);
-    c.TV[n] = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
-    c.TA[n] = make_int4(oDC, oCA, enc(t, 1), 0);
-    if (oBD >= 0) ((int*)&c.TA[oBD >> 2])[oBD & 3] = enc(t, 0);
-    if (oAB >= 0) ((int*)&c.TA[oAB >> 2])[oAB & 3] = enc(t, 2);
-    if (oDC >= 0) ((int*)&c.TA[oDC >> 2])[oDC & 3] = enc(n, 0);
-    if (oCA >= 0) ((int*)&c.TA[oCA >> 2])[oCA & 3] = enc(n, 1);
+    tri_v(c, t) = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
+    tri_a(c, t) = make_int4(oBD, enc(n, 2), oAB, 0);
+    tri_v(c, n) = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
+    tri_a(c, n) = make_int4(oDC, oCA, enc(t, 1), 0);
+    if (oBD >= 0) ((int*)&tri_a(c, oBD >> 2))[oBD & 3] = enc(t, 0);
+    if (oAB >= 0) ((int*)&tri_a(c, oAB >> 2))[oAB & 3] = enc(t, 2);
+    if (oDC >= 0) ((int*)&tri_a(c, oDC >> 2))[oDC & 3] = enc(n, 0);
+    if (oCA >= 0) ((int*)&tri_a(c, oCA >> 2))[oCA & 3] = enc(n, 1);
     c.vt[A] = t; c.vt[B] = t; c.vt[D] = t; c.vt[C] = n;
     return n;
 }
@@ -891,7 +896,7 @@ GCDT_HD void body_cproc(const Ctx& c, int k) {
     // crossing edges between consecutive chain triangles
     int qn = 0;
     for (int m = 0; m + 1 < kt; ++m) {
-        int4 ta = c.TA[L[m]];
+        int4 ta = tri_a(c, L[m]);
         int s = (ta.x >> 2) == L[m + 1] ? 0 : ((ta.y >> 2) == L[m + 1] ? 1 : 2);
         Q[qn++] = enc(L[m], s);
     }
@@ -901,11 +906,11 @@ GCDT_HD void body_cproc(const Ctx& c, int k) {
         if (++guard > limit) { fail(c, ST_ITER_LIMIT); return; }
         int e = Q[head]; head = head + 1 == kt ? 0 : head + 1; size--;
         int t = e >> 2, i = e & 3;
-        int4 tv = c.TV[t];
-        int en = comp(c.TA[t], i);
+        int4 tv = tri_v(c, t);
+        int en = comp(tri_a(c, t), i);
         int n = en >> 2, j = en & 3;
         int A = comp(tv, i), B = comp(tv, nx3(i)), C = comp(tv, nx3(nx3(i)));
-        int D = comp(c.TV[n], j);
+        int D = comp(tri_v(c, n), j);
         int2 PA = c.P[A], PD = c.P[D];
         int s1 = orient2d(PA, PD, c.P[B]), s2 = orient2d(PA, PD, c.P[C]);
         int tail = head + size; if (tail >= kt) tail -= kt;
@@ -924,7 +929,7 @@ GCDT_HD void body_cproc(const Ctx& c, int k) {
     }
     // flag the recovered edge (a, stop) on both sides
     for (int m = 0; m < kt; ++m) {
-        int4 tv = c.TV[L[m]];
+        int4 tv = tri_v(c, L[m]);
         bool ha = tv.x == a || tv.y == a || tv.z == a;
         bool hs = tv.x == stop || tv.y == stop || tv.z == stop;
         if (ha && hs) {
@@ -941,7 +946,7 @@ GCDT_HD void body_cproc(const Ctx& c, int k) {
 // ---------------------------------------------------------------- output
 
 GCDT_HD void body_output(const Ctx& c, int t) {
-    int4 tv = c.TV[t], ta = c.TA[t];
+    int4 tv = tri_v(c, t), ta = tri_a(c, t);
     c.out_tris[3 * t + 0] = c.perm[tv.x];
     c.out_tris[3 * t + 1] = c.perm[tv.y];
     c.out_tris[3 * t + 2] = c.perm[tv.z];

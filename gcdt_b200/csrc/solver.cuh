@@ -47,8 +47,7 @@ __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     c.P = (int2*)(base + p.o_P);
     c.perm = (int*)(base + p.o_perm);
     c.rank = (int*)(base + p.o_rank);
-    c.TV = (int4*)(base + p.o_TV);
-    c.TA = (int4*)(base + p.o_TA);
+    c.tri = (int4*)(base + p.o_tri);
     c.loc = (int*)(base + p.o_loc);
     c.pedge = (signed char*)(base + p.o_pedge);
     c.act = (int*)(base + p.o_actA);
@@ -74,9 +73,9 @@ __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     c.lvl = (unsigned char*)(base + p.o_lvl);
     c.cnt = (Counters*)(base + p.o_cnt);
     // three levels: every 512th point of the Morton order plus all segment
-    // endpoints, then every 32nd, then the rest
+    // endpoints, then every 8th, then the rest
     c.nlevels = 3;
-    c.stride[0] = 512; c.stride[1] = 32; c.stride[2] = 1; c.stride[3] = 1;
+    c.stride[0] = 512; c.stride[1] = 8; c.stride[2] = 1; c.stride[3] = 1;
     return c;
 }
 
