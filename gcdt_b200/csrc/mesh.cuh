@@ -8,7 +8,8 @@
 //   tri[2t]   int4   TV: (v0, v1, v2, cflags) -- CCW vertices, bit k of .w set
 //                    when the edge opposite v_k is a constraint edge
 //   tri[2t+1] int4   TA: (a0, a1, a2, -)  a_k = 4*n + j: neighbour n across the
-//                    edge opposite v_k, which is opposite slot j in n; -1 = box
+//                    edge opposite v_k, which is opposite slot j in n; -1 = box;
+//                    .w = the insertion round that last changed the triangle
 //                    (TV and TA of a triangle share one 32-byte sector: most
 //                    visits read both)
 // Triangle slots never move: the two root triangles are 0 and 1, and sorted
@@ -105,13 +106,11 @@ struct Ctx {
     int* act_next;            // active point list (append)
     unsigned long long* vote; // per triangle: (round<<32) | ~hash(point)
     int2* ins;                // per triangle: (round, 8*q + split code)
-    int* modR;                // per triangle: last round it changed
     int2* winners;            // (q, t) inserted this round
 
     unsigned long long* claim;  // per triangle: (stamp<<32) | ~key
     int2* cand;                 // per queue entry: (4t+i, 4n+j) or (-1,-1)
-    int4* fmap;                 // per flipped triangle: old slot -> new (4t+s)
-    int* fst;                   // per triangle: sub-round it was flipped
+    int4* fmap;                 // per flipped triangle: old slot -> new (4t+s), .w = sub-round of the flip
     int* qst;                   // per triangle: queue stamp (dedup)
     int* queue;                 // flip queue (read)
     int* queue_next;            // flip queue (append)
@@ -289,8 +288,7 @@ GCDT_HD void body_clear(const Ctx& c, int t) {
     c.vote[t] = 0;
     c.claim[t] = 0;
     c.ins[t] = make_int2(0, 0);
-    c.modR[t] = -1;
-    c.fst[t] = -1;
+    c.fmap[t] = make_int4(-1, -1, -1, -1);
     c.qst[t] = 0;
 }
 
@@ -463,7 +461,7 @@ GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
     int t = c.loc[q];
     if (t < 0) return;                       // inserted last round
     int2 p = c.P[q];
-    if (c.modR[t] == (int)c.round - 1) {
+    if (tri_a(c, t).w == (int)c.round - 1) {
         int steps = 0;
         int nt = walk(c, t, p, 256, &steps);
         if (nt < 0) nt = locate_from_vertex(c, tri_v(c, t).x, t, p);
@@ -503,14 +501,13 @@ GCDT_HD void body_split(const Ctx& c, int k) {
         for (int j = 0; j < 3; ++j) {
             int4 v = tv; setc(v, j, q); v.w = fl & (1 << j);
             int4 a;
-            a.w = 0;
+            a.w = (int)c.round;
             for (int kk = 0; kk < 3; ++kk)
                 setc(a, kk, kk == j ? comp(ta, j) : enc(ch[kk], j));
             tri_v(c, ch[j]) = v;
             tri_a(c, ch[j]) = a;
         }
         c.ins[t] = make_int2((int)c.round, q * 8 + 7);
-        c.modR[t] = (int)c.round;
     } else {
         int en = comp(ta, e);
         int n = en >> 2, e2 = en & 3;
@@ -524,28 +521,26 @@ GCDT_HD void body_split(const Ctx& c, int k) {
         int4 v, a;
         // A1
         v = tv; setc(v, e1, q); v.w = fl & ((1 << e1) | (1 << e));
-        a = make_int4(0, 0, 0, 0);
+        a = make_int4(0, 0, 0, (int)c.round);
         setc(a, e1, comp(ta, e1)); setc(a, e_2, enc(A2, e1)); setc(a, e, enc(B2, e2));
         tri_v(c, A1) = v; tri_a(c, A1) = a;
         // A2
         v = tv; setc(v, e_2, q); v.w = fl & ((1 << e_2) | (1 << e));
-        a = make_int4(0, 0, 0, 0);
+        a = make_int4(0, 0, 0, (int)c.round);
         setc(a, e_2, comp(ta, e_2)); setc(a, e1, enc(A1, e_2)); setc(a, e, enc(B1, e2));
         tri_v(c, A2) = v; tri_a(c, A2) = a;
         // B1
         v = nv; setc(v, f1, q); v.w = gl & ((1 << f1) | (1 << e2));
-        a = make_int4(0, 0, 0, 0);
+        a = make_int4(0, 0, 0, (int)c.round);
         setc(a, f1, comp(na, f1)); setc(a, f2, enc(B2, f1)); setc(a, e2, enc(A2, e));
         tri_v(c, B1) = v; tri_a(c, B1) = a;
         // B2
         v = nv; setc(v, f2, q); v.w = gl & ((1 << f2) | (1 << e2));
-        a = make_int4(0, 0, 0, 0);
+        a = make_int4(0, 0, 0, (int)c.round);
         setc(a, f2, comp(na, f2)); setc(a, f1, enc(B1, f2)); setc(a, e2, enc(A1, e));
         tri_v(c, B2) = v; tri_a(c, B2) = a;
         c.ins[t] = make_int2((int)c.round, q * 8 + e);
         c.ins[n] = make_int2((int)c.round, q * 8 + 3 + e2);
-        c.modR[t] = (int)c.round;
-        c.modR[n] = (int)c.round;
     }
     c.loc[q] = -1;
     c.winners[append_slot(&c.cnt->cur_win, c.base_win)] = make_int2(q, t);
@@ -662,18 +657,14 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     int A = comp(tv, i), B = comp(tv, i1), C = comp(tv, i2), D = comp(nv, j);
     int ft = tv.w, fn = nv.w;
     tri_v(c, t) = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
-    tri_a(c, t) = make_int4(comp(na, j1), enc(n, 2), comp(ta, i2), 0);
+    tri_a(c, t) = make_int4(comp(na, j1), enc(n, 2), comp(ta, i2), (int)c.round);
     tri_v(c, n) = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
-    tri_a(c, n) = make_int4(comp(na, j2), comp(ta, i1), enc(t, 1), 0);
-    int4 mt = make_int4(-1, -1, -1, 0), mn = make_int4(-1, -1, -1, 0);
+    tri_a(c, n) = make_int4(comp(na, j2), comp(ta, i1), enc(t, 1), (int)c.round);
+    int4 mt = make_int4(-1, -1, -1, (int)c.sr), mn = make_int4(-1, -1, -1, (int)c.sr);
     setc(mt, i1, enc(n, 1)); setc(mt, i2, enc(t, 2));
     setc(mn, j1, enc(t, 0)); setc(mn, j2, enc(n, 0));
     c.fmap[t] = mt;
     c.fmap[n] = mn;
-    c.fst[t] = (int)c.sr;
-    c.fst[n] = (int)c.sr;
-    c.modR[t] = (int)c.round;
-    c.modR[n] = (int)c.round;
     // The new diagonal AD is locally Delaunay: queue the four outer edges.
     // Flip number f of the sub-round owns entries 2f, 2f+1 of the next
     // queue; body_flip_fix reads the pairs from there and appends the
@@ -688,8 +679,9 @@ GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
     int old = comp(*row, s);
     if (old < 0) return;
     int m = old >> 2, ms = old & 3;
-    if (c.fst[m] == (int)c.sr) {
-        ((int*)row)[s] = comp(c.fmap[m], ms);
+    int4 fm = c.fmap[m];
+    if (fm.w == (int)c.sr) {
+        ((int*)row)[s] = comp(fm, ms);
     } else {
         ((int*)&tri_a(c, m))[ms] = enc(tt, s);
     }
@@ -702,7 +694,7 @@ GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
 GCDT_HD void body_flip_fix(const Ctx& c, int k) {
     if (k >= c.list_n) {
         int2 cd = c.cand[k - c.list_n];
-        if (cd.x >= 0 && c.fst[cd.x >> 2] != (int)c.sr)
+        if (cd.x >= 0 && c.fmap[cd.x >> 2].w != (int)c.sr)
             c.queue_next[2 * c.list_n + append_slot(&c.cnt->cur_q, c.base_q)] = c.queue[k - c.list_n];
         return;
     }
@@ -857,9 +849,9 @@ GCDT_HD int flip_local(const Ctx& c, int t, int i) {
     int ft = tv.w, fn = nv.w;
     int oBD = comp(na, j1), oAB = comp(ta, i2), oDC = comp(na, j2), oCA = comp(ta, i1);
     tri_v(c, t) = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
-    tri_a(c, t) = make_int4(oBD, enc(n, 2), oAB, 0);
+    tri_a(c, t) = make_int4(oBD, enc(n, 2), oAB, (int)c.round);
     tri_v(c, n) = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
-    tri_a(c, n) = make_int4(oDC, oCA, enc(t, 1), 0);
+    tri_a(c, n) = make_int4(oDC, oCA, enc(t, 1), (int)c.round);
     if (oBD >= 0) ((int*)&tri_a(c, oBD >> 2))[oBD & 3] = enc(t, 0);
     if (oAB >= 0) ((int*)&tri_a(c, oAB >> 2))[oAB & 3] = enc(t, 2);
     if (oDC >= 0) ((int*)&tri_a(c, oDC >> 2))[oDC & 3] = enc(n, 0);
