@@ -16,7 +16,7 @@ namespace gcdt {
 // grid-stride loops separated by a grid barrier, so the round structure
 // costs no kernel launches and no host round trips.
 
-constexpr int kPersistBlock = 256;
+constexpr int kPersistBlock = 512;   // one block per SM (128 registers per thread)
 
 struct GridExec {
     static constexpr bool kCanNarrow = true;

@@ -39,7 +39,7 @@ __global__ void gcdt_predicates(const int2* q, int n, int* out) {
 
 static_assert(offsetof(Counters, cur_scr) + 8 <= GridExec::kSnapWords * 8, "cursors are in the snapshot");
 
-__global__ void __launch_bounds__(kPersistBlock, 2) gcdt_stages(Ctx c) {
+__global__ void __launch_bounds__(kPersistBlock, 1) gcdt_stages(Ctx c) {
     __shared__ unsigned long long snap[GridExec::kSnapWords];
     GridExec ex{c.cnt, gridDim.x, snap};
     if (threadIdx.x == 0) ex.take_snapshot();

@@ -432,24 +432,35 @@ GCDT_HD void body_vt_live(const Ctx& c, int k) {
 
 // Visibility walk from t to the triangle whose closed interior holds p.
 // Terminates in a Delaunay triangulation (acyclic in-front-of relation).
-GCDT_HD int walk(const Ctx& c, int t, int2 p, int limit, int* steps) {
+// On success *edge is the slot of the edge p lies on, or -1 (p is not a
+// vertex, so it lies on at most one edge).
+GCDT_HD int walk(const Ctx& c, int t, int2 p, int limit, int* edge) {
     for (int it = 0; it < limit; ++it) {
         int4 tv = tri_v(c, t);
         int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
-        int side = -1;
+        int side = -1, zero = -1;
         int r = it % 3;
         for (int k = 0; k < 3 && side < 0; ++k) {
             int s = r + k; if (s >= 3) s -= 3;
             int o = s == 0 ? orient2d(b, cc, p) : (s == 1 ? orient2d(cc, a, p) : orient2d(a, b, p));
             if (o < 0) side = s;
+            else if (o == 0) zero = s;
         }
-        if (side < 0) { *steps += it; return t; }
+        if (side < 0) { *edge = zero; return t; }
         int nb = comp(tri_a(c, t), side);
-        if (nb < 0) { *steps += it; return -1; }
+        if (nb < 0) return -1;
         t = nb >> 2;
     }
-    *steps += limit;
     return -1;
+}
+
+// Slot of the edge of t that p lies on, or -1; flags p outside t.
+GCDT_HD int edge_of(const Ctx& c, int t, int2 p) {
+    int4 tv = tri_v(c, t);
+    int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
+    int o0 = orient2d(b, cc, p), o1 = orient2d(cc, a, p), o2 = orient2d(a, b, p);
+    if (o0 < 0 || o1 < 0 || o2 < 0) fail(c, ST_INTERNAL);
+    return o0 == 0 ? 0 : (o1 == 0 ? 1 : (o2 == 0 ? 2 : -1));
 }
 
 // Active point: relocate if its triangle changed in the previous round,
@@ -461,20 +472,20 @@ GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
     int t = c.loc[q];
     if (t < 0) return;                       // inserted last round
     int2 p = c.P[q];
+    int e;
     if (tri_a(c, t).w == (int)c.round - 1) {
-        int steps = 0;
-        int nt = walk(c, t, p, 256, &steps);
-        if (nt < 0) nt = locate_from_vertex(c, tri_v(c, t).x, t, p);
-        if (nt < 0) { fail(c, ST_ITER_LIMIT); return; }
+        int nt = walk(c, t, p, 256, &e);
+        if (nt < 0) {
+            nt = locate_from_vertex(c, tri_v(c, t).x, t, p);
+            if (nt < 0) { fail(c, ST_ITER_LIMIT); return; }
+            e = edge_of(c, nt, p);
+        }
         t = nt;
         c.loc[q] = t;
+    } else {
+        e = edge_of(c, t, p);
     }
     c.act_next[append_slot(&c.cnt->cur_act, c.base_act)] = q;
-    int4 tv = tri_v(c, t);
-    int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
-    int o0 = orient2d(b, cc, p), o1 = orient2d(cc, a, p), o2 = orient2d(a, b, p);
-    int e = o0 == 0 ? 0 : (o1 == 0 ? 1 : (o2 == 0 ? 2 : -1));
-    if (o0 < 0 || o1 < 0 || o2 < 0) fail(c, ST_INTERNAL);
     c.pedge[q] = (signed char)e;
     unsigned long long key = ((unsigned long long)c.round << 32) | (0xffffffffu - hash32((uint32_t)q));
     if (c.vote[t] < key) at_max64(&c.vote[t], key);
