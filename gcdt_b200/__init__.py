@@ -74,6 +74,10 @@ def lib():
     L.gcdt_workspace_bytes.restype = ctypes.c_size_t
     L.gcdt_triangulate.argtypes = [vp, vp, i32, vp, i32, vp, vp, vp, ctypes.POINTER(i32), vp]
     L.gcdt_triangulate.restype = ctypes.c_int
+    L.gcdt_triangulate_async.argtypes = [vp, vp, i32, vp, i32, vp, vp, vp, vp]
+    L.gcdt_triangulate_async.restype = ctypes.c_int
+    L.gcdt_wait.argtypes = [vp, ctypes.POINTER(i32)]
+    L.gcdt_wait.restype = ctypes.c_int
     L.gcdt_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     L.gcdt_get_stats.restype = ctypes.c_int
     L.gcdt_status_string.argtypes = [ctypes.c_int]
@@ -216,8 +220,7 @@ class Triangulator:
                                       ctypes.c_void_p(d_cflags), ctypes.byref(nt),
                                       ctypes.c_void_p(stream))
 
-    def triangulate(self, points, segments=None, out=None, stream=None):
-        """Device tensors in, device tensors out: (tris (T,3), adj (T,3), cflags (T,))."""
+    def _args(self, points, segments, out, stream):
         import torch
         if points.dtype != torch.int32 or not points.is_cuda:
             raise TypeError("points must be a CUDA int32 tensor of shape (n, 2)")
@@ -240,11 +243,48 @@ class Triangulator:
             tris, adj, cflags = out
         if stream is None:
             stream = torch.cuda.current_stream(points.device).cuda_stream
+        return points, segments, n, sp, s, (tris, adj, cflags), stream
+
+    def triangulate(self, points, segments=None, out=None, stream=None):
+        """Device tensors in, device tensors out: (tris (T,3), adj (T,3), cflags (T,))."""
+        points, segments, n, sp, s, out, stream = self._args(points, segments, out, stream)
+        tris, adj, cflags = out
         rc = self.triangulate_raw(points.data_ptr() if n else 0, n, sp, s,
                                   tris.data_ptr(), adj.data_ptr(), cflags.data_ptr(), stream)
         if rc != 0:
             raise GcdtError(rc, "gcdt_triangulate")
         return tris, adj, cflags
+
+    def triangulate_async(self, points, segments=None, out=None, stream=None):
+        """Enqueue a solve on `stream` (default: the current stream) and return
+        the output tensors at once; wait() reports the solve's status.  The
+        inputs and outputs are kept referenced until then.  One solve in
+        flight per Triangulator: a further call waits for the previous one."""
+        if getattr(self, "_inflight", None) is not None:
+            self.wait()
+        points, segments, n, sp, s, out, stream = self._args(points, segments, out, stream)
+        tris, adj, cflags = out
+        rc = lib().gcdt_triangulate_async(self._h, ctypes.c_void_p(points.data_ptr() if n else 0), int(n),
+                                          ctypes.c_void_p(sp or 0), int(s),
+                                          ctypes.c_void_p(tris.data_ptr()), ctypes.c_void_p(adj.data_ptr()),
+                                          ctypes.c_void_p(cflags.data_ptr()), ctypes.c_void_p(stream))
+        if rc != 0:
+            self.wait()
+            raise GcdtError(rc, "gcdt_triangulate_async")
+        self._inflight = (points, segments, out)
+        return out
+
+    def wait(self):
+        """Block until the solve enqueued by triangulate_async is done; raise
+        GcdtError if it failed.  Returns the triangle count (0 if none was
+        in flight)."""
+        nt = ctypes.c_int32(0)
+        busy = getattr(self, "_inflight", None) is not None
+        rc = lib().gcdt_wait(self._h, ctypes.byref(nt))
+        self._inflight = None
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_wait")
+        return int(nt.value) if busy else 0
 
     def triangulate_host(self, points, segments=None):
         """numpy in, numpy out (copies to and from the device)."""

@@ -139,6 +139,11 @@ struct gcdt_context {
     Counters* hcnt = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     gcdt_stats stats{};
+    // the solve enqueued by gcdt_triangulate_async, until gcdt_wait
+    bool pending = false;
+    int32_t pend_n = 0, pend_s = 0;
+    long long pend_launches = 0;
+    cudaError_t pend_err = cudaSuccess;
 };
 
 namespace {
@@ -190,6 +195,7 @@ extern "C" gcdt_status gcdt_create(gcdt_context** out, int device, int64_t max_p
 extern "C" void gcdt_destroy(gcdt_context* ctx) {
     if (!ctx) return;
     DeviceGuard g(ctx->device);
+    if (ctx->pending) cudaEventSynchronize(ctx->ev1);   // a solve still writes the arena
     if (ctx->arena) cudaFree(ctx->arena);
     if (ctx->hcnt) cudaFreeHost(ctx->hcnt);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -197,14 +203,15 @@ extern "C" void gcdt_destroy(gcdt_context* ctx) {
     delete ctx;
 }
 
-extern "C" gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_points, int32_t n,
-                                        const int32_t* d_segments, int32_t s,
-                                        int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
-                                        int32_t* n_tris, void* stream) {
+extern "C" gcdt_status gcdt_triangulate_async(gcdt_context* ctx, const int32_t* d_points, int32_t n,
+                                              const int32_t* d_segments, int32_t s,
+                                              int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                              void* stream) {
     if (!ctx || n < 0 || s < 0 || (n > 0 && !d_points) || (s > 0 && !d_segments) ||
         !d_tris || !d_adj || !d_cflags)
         return GCDT_BAD_INPUT;
     if (n > ctx->max_n || s > ctx->max_s) return GCDT_OOM;
+    if (ctx->pending) gcdt_wait(ctx, nullptr);   // one solve in flight per context
     DeviceGuard g(ctx->device);
     Plan plan = make_plan(n, s, sort_temp_bytes(n));
     if (plan.L.total > ctx->arena_bytes) return GCDT_OOM;
@@ -220,28 +227,60 @@ extern "C" gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_poin
     bk.hcnt = ctx->hcnt;
     bk.sort_tmp = ctx->arena + plan.o_sort_tmp;
     bk.sort_bytes = plan.sort_temp_bytes;
+    bk.note(cudaEventRecord(ctx->ev0, bk.st));
+    enqueue_solve(bk, c);
+    bk.note(cudaMemcpyAsync(ctx->hcnt, c.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, bk.st));
+    bk.note(cudaEventRecord(ctx->ev1, bk.st));
+    ctx->pending = true;
+    ctx->pend_n = n;
+    ctx->pend_s = s;
+    ctx->pend_launches = bk.launches;
+    ctx->pend_err = bk.err;
+    return bk.err == cudaSuccess ? GCDT_OK : GCDT_CUDA_ERROR;
+}
+
+extern "C" gcdt_status gcdt_wait(gcdt_context* ctx, int32_t* n_tris) {
+    if (!ctx) return GCDT_BAD_INPUT;
+    if (!ctx->pending) return GCDT_OK;
+    DeviceGuard g(ctx->device);
+    ctx->pending = false;
+    cudaError_t e = cudaEventSynchronize(ctx->ev1);
     SolveStats st;
-    cudaEventRecord(ctx->ev0, bk.st);
-    int bits = run_solve(bk, c, st);
-    cudaEventRecord(ctx->ev1, bk.st);
-    bk.note(cudaEventSynchronize(ctx->ev1));
-    if (bk.err != cudaSuccess) bits |= ST_CUDA;
+    int bits = solve_result(*ctx->hcnt, st);
+    if (e != cudaSuccess || ctx->pend_err != cudaSuccess) {
+        cudaGetLastError();
+        bits |= ST_CUDA;
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    const int32_t n = ctx->pend_n;
     gcdt_stats& S = ctx->stats;
     S.n_points = n;
-    S.n_segments = s;
+    S.n_segments = ctx->pend_s;
     S.n_triangles = 2 * (int64_t)n + 2;
     S.insertion_rounds = st.rounds;
     S.flip_subrounds = st.flip_subrounds;
     S.flips = st.flips;
     S.constraint_rounds = st.constraint_rounds;
-    S.host_syncs = st.host_syncs;
-    S.kernel_launches = bk.launches;
+    S.host_syncs = 1;
+    S.kernel_launches = ctx->pend_launches;
     S.device_ms = ms;
     gcdt_status rc = map_status(bits);
     if (rc == GCDT_OK && n_tris) *n_tris = 2 * n + 2;
     return rc;
+}
+
+extern "C" gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_points, int32_t n,
+                                        const int32_t* d_segments, int32_t s,
+                                        int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                        int32_t* n_tris, void* stream) {
+    if (ctx && ctx->pending) gcdt_wait(ctx, nullptr);
+    gcdt_status rc = gcdt_triangulate_async(ctx, d_points, n, d_segments, s, d_tris, d_adj, d_cflags, stream);
+    if (rc != GCDT_OK) {
+        if (ctx && ctx->pending) gcdt_wait(ctx, nullptr);
+        return rc;
+    }
+    return gcdt_wait(ctx, n_tris);
 }
 
 extern "C" gcdt_status gcdt_get_stats(const gcdt_context* ctx, gcdt_stats* out) {

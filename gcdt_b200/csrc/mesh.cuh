@@ -632,23 +632,29 @@ GCDT_HD void body_flip_check(const Ctx& c, int k) {
     int qe = c.queue[k];
     int t = qtri(qe), mask = qe & 7;
     int4 tv = tri_v(c, t), ta = tri_a(c, t);
+    // the edges to test: in the mask, with a neighbour, not constraints
+    int live = mask & ~tv.w & ((ta.x >= 0) | ((ta.y >= 0) << 1) | ((ta.z >= 0) << 2));
+    // issue every test's loads before the first test, so the neighbour rows
+    // and the opposite points of up to three edges are in flight together
+    int d0 = 0, d1 = 0, d2 = 0;
+    if (live & 1) d0 = comp(tri_v(c, ta.x >> 2), ta.x & 3);
+    if (live & 2) d1 = comp(tri_v(c, ta.y >> 2), ta.y & 3);
+    if (live & 4) d2 = comp(tri_v(c, ta.z >> 2), ta.z & 3);
     int2 a = c.P[tv.x], b = c.P[tv.y], cc = c.P[tv.z];
-    for (int i = 0; i < 3; ++i) {
-        if (!((mask >> i) & 1)) continue;
-        int en = comp(ta, i);
-        if (en < 0 || ((tv.w >> i) & 1)) continue;
-        int n = en >> 2, j = en & 3;
-        int d = comp(tri_v(c, n), j);
-        if (incircle_sos(a, b, cc, c.P[d]) > 0) {
-            int key = enc(t, i);
-            unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)key));
-            at_max64(&c.claim[t], ck);
-            at_max64(&c.claim[n], ck);
-            c.cand[k] = make_int2(key, en);
-            return;
-        }
-    }
-    c.cand[k] = make_int2(-1, -1);
+    int2 p0 = c.P[d0], p1 = c.P[d1], p2 = c.P[d2];
+    // first edge in slot order that is not locally Delaunay
+    int i = -1;
+    if ((live & 1) && incircle_sos(a, b, cc, p0) > 0) i = 0;
+    else if ((live & 2) && incircle_sos(a, b, cc, p1) > 0) i = 1;
+    else if ((live & 4) && incircle_sos(a, b, cc, p2) > 0) i = 2;
+    if (i < 0) { c.cand[k] = make_int2(-1, -1); return; }
+    int en = comp(ta, i);
+    int n = en >> 2;
+    int key = enc(t, i);
+    unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)key));
+    at_max64(&c.claim[t], ck);
+    at_max64(&c.claim[n], ck);
+    c.cand[k] = make_int2(key, en);
 }
 
 // Winners flip: t=(A,B,C) with A in slot i, n=(D,C,B) with D in slot j

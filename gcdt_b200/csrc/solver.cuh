@@ -263,6 +263,11 @@ GCDT_HD int run_stages(EX& ex, Ctx c) {
     D.round = 0; D.sr = 0; D.rounds = 0; D.subrounds = 0; D.crounds = 0;
     D.e_act0 = D.e_act = D.e_win = D.e_q = D.e_flip = D.e_pend = D.e_law = D.e_scr = 0;
     D.nphase = 0; D.errs = 0;
+    // set-up (keys, gather, segments) flagged bad input: stop before any phase
+    if (ex.word(&c.cnt->status) | ex.word(&c.cnt->err[0]) | ex.word(&c.cnt->err[1])) {
+        ex.finish(c, 0, 0, 0, 0);
+        return ST_BAD_INPUT;
+    }
     int rc = 0;
     for (int l = 0; l < c.nlevels && n > 0 && rc == 0; ++l) {
         c.level = l;
@@ -289,9 +294,10 @@ GCDT_HD int run_stages(EX& ex, Ctx c) {
 
 // Host part: clear the per-solve arrays, Morton sort, gather, levels and
 // segment set-up, then hand over to the stages (one persistent kernel on the
-// GPU).
+// GPU).  Everything is enqueued on the backend's stream without waiting:
+// errors found by the set-up kernels make the stage kernel stop at once.
 template <class BK>
-int run_solve(BK& bk, Ctx c, SolveStats& st) {
+void enqueue_solve(BK& bk, Ctx c) {
     const int n = c.n;
     const long long T = c.ntri;
     bk.fill(c.cnt, 0, sizeof(Counters));
@@ -311,16 +317,26 @@ int run_solve(BK& bk, Ctx c, SolveStats& st) {
         bk.launch(K_SEG_INIT, c, c.s);
         bk.launch(K_SEG_LEVEL0, c, c.s);
     }
-    Counters h;
-    bk.read(&h); st.host_syncs++;
-    if (h.status | h.err[0] | h.err[1]) return h.status | h.err[0] | h.err[1];
     bk.stages(c);
-    bk.read(&h); st.host_syncs++;
+}
+
+// Status bits and statistics of a finished solve from its counters.
+inline int solve_result(const Counters& h, SolveStats& st) {
     st.rounds = h.rounds;
     st.flip_subrounds = h.flip_subrounds;
     st.constraint_rounds = h.constraint_rounds;
     st.flips = (long long)h.cur_flip;
     return h.status | h.err[0] | h.err[1];
+}
+
+// One solve, then one read of the counters.
+template <class BK>
+int run_solve(BK& bk, Ctx c, SolveStats& st) {
+    enqueue_solve(bk, c);
+    Counters h;
+    bk.read(&h);
+    st.host_syncs++;
+    return solve_result(h, st);
 }
 
 }  // namespace gcdt

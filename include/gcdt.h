@@ -85,6 +85,24 @@ gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_points, int32_t
                              int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
                              int32_t* n_tris, void* stream);
 
+/* The same solve, enqueued on `stream` without waiting for it: returns once
+   the work is queued (GCDT_OK), or with the argument / capacity error.  The
+   solve's own status (bad input found on the device, crossing constraints,
+   iteration limits) comes from gcdt_wait, which blocks until the solve is
+   done; statistics and the phase profile are those of the last waited
+   solve.  A context holds one solve in flight: a further call on it first
+   waits for the previous one.  With two contexts on two streams a caller
+   keeps the GPU busy while one solve's input and output copies run.
+   (The reference runs its stages synchronously, kernel.cu:5395-5448.) */
+gcdt_status gcdt_triangulate_async(gcdt_context* ctx, const int32_t* d_points, int32_t n,
+                                   const int32_t* d_segments, int32_t s,
+                                   int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                   void* stream);
+/* Wait for the solve enqueued by gcdt_triangulate_async and return its
+   status; *n_tris (host, may be NULL) receives 2n+2 on success.  GCDT_OK at
+   once when nothing is in flight. */
+gcdt_status gcdt_wait(gcdt_context* ctx, int32_t* n_tris);
+
 gcdt_status gcdt_get_stats(const gcdt_context* ctx, gcdt_stats* out);
 const char* gcdt_status_string(gcdt_status s);
 
