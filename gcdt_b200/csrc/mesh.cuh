@@ -85,6 +85,7 @@ struct Ctx {
     int eslot;      // error word of the running phase (phase parity)
     unsigned lawson_sr;  // queue stamp of the constrained flip pass
     int list_n;     // length of the list a launch iterates over
+    int carry_n;    // leading flip-queue entries carried over from the previous round
 
     const int2* in_xy;
     const int2* in_cons;
@@ -631,6 +632,9 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
 GCDT_HD void body_flip_check(const Ctx& c, int k) {
     int qe = c.queue[k];
     int t = qtri(qe), mask = qe & 7;
+    // a carried entry whose triangle was split this round: the split's own
+    // queue entries test every old edge of it
+    if (k < c.carry_n && c.ins[t].x == (int)c.round) { c.cand[k] = make_int2(-1, -1); return; }
     int4 tv = tri_v(c, t), ta = tri_a(c, t);
     // the edges to test: in the mask, with a neighbour, not constraints
     int live = mask & ~tv.w & ((ta.x >= 0) | ((ta.y >= 0) << 1) | ((ta.z >= 0) << 2));
