@@ -9,7 +9,10 @@ workload (10,000,000 generated points -- 90% from 64 Gaussians, sigma 2^22,
 `value` = points triangulated per second over all ranks (Mpts/s).
 `e2e` = the same metric through the public API from pinned host buffers,
 with the host->device copy of points and segments and the device->host copy
-of triangles, adjacency and flags inside the timed region.
+of triangles, adjacency and flags inside the timed region, for a stream of
+inputs double-buffered over two contexts and two streams
+(gcdt_triangulate_async: solves in order, copies overlapped); e2e.serial is
+the one-step-at-a-time figure.
 
 N > 1 runs independent replicas, one per rank (the path has no data-parallel
 exchange: a single triangulation stays on one GPU), so scaling is weak.
@@ -38,9 +41,9 @@ WORKLOAD = "plain CDT at scale: 10M Gaussian-mixture/uniform int32 points in [1,
 CPU_SAMPLE_POINTS = 2_000_000   # config-shaped sample for the CPU legs (18x18 polygon grid, 632 polygons)
 # DRAM bytes (read + write) of the stage kernel per point, from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the same workload shape at
-# 1,020,608 points: 1,854,183,936 + 1,068,919,552 bytes.  Reported per solve as
-# this figure times N (the full-size capture would replay a 3 GB arena ~40x).
-DRAM_BYTES_PER_POINT = (1854183936 + 1068919552) / 1020608
+# 1,020,608 points: 1,861,193,984 + 903,404,544 bytes.  Reported per solve as
+# this figure times N (the full-size capture would replay a 2.9 GB arena ~40x).
+DRAM_BYTES_PER_POINT = (1861193984 + 903404544) / 1020608
 
 
 def rank_info():
