@@ -72,8 +72,17 @@ struct GridExec {
         long long t0 = timer ? clock64() : 0;
         if (!(word(&cnt->status) & ST_BARRIER)) {
             long long stride = (long long)gridDim.x * blockDim.x;
-            for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
-                dispatch(k, c, (int)i);
+            long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            // latency-bound passes: two items per thread and trip (i, i + stride)
+            if (k == K_FLIP_CHECK) {
+                for (; i < count; i += 2 * stride)
+                    body_flip_check_pair(c, (int)i, i + stride < count ? (int)(i + stride) : -1);
+            } else if (k == K_FLIP_FIX) {
+                for (; i < count; i += 2 * stride)
+                    body_flip_fix_pair(c, (int)i, i + stride < count ? (int)(i + stride) : -1);
+            } else {
+                for (; i < count; i += stride) dispatch(k, c, (int)i);
+            }
         }
         barrier();
         if (timer && k < kMaxPhaseKinds) {   // phase time incl. the barrier, as block 0 sees it

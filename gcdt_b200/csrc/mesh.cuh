@@ -661,19 +661,73 @@ GCDT_HD void body_flip_check(const Ctx& c, int k) {
     c.cand[k] = make_int2(key, en);
 }
 
+// Two queue entries per thread (k1 < 0: only k0), each stage's loads issued
+// for both entries before either is used: twice the loads in flight per
+// thread for this latency-bound pass.  Same result as body_flip_check on
+// each entry.
+GCDT_HD void body_flip_check_pair(const Ctx& c, int k0, int k1) {
+    const int ks[2] = {k0, k1};
+    bool on[2];
+    int t[2], mask[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        on[u] = ks[u] >= 0;
+        int qe = on[u] ? c.queue[ks[u]] : 0;
+        t[u] = qtri(qe);
+        mask[u] = qe & 7;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+        if (on[u] && ks[u] < c.carry_n && c.ins[t[u]].x == (int)c.round) on[u] = false;
+    int4 tv[2], ta[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        tv[u] = on[u] ? tri_v(c, t[u]) : make_int4(0, 0, 0, 7);
+        ta[u] = on[u] ? tri_a(c, t[u]) : make_int4(-1, -1, -1, 0);
+    }
+    int live[2], d[2][3];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        live[u] = mask[u] & ~tv[u].w & ((ta[u].x >= 0) | ((ta[u].y >= 0) << 1) | ((ta[u].z >= 0) << 2));
+        d[u][0] = (live[u] & 1) ? comp(tri_v(c, ta[u].x >> 2), ta[u].x & 3) : 0;
+        d[u][1] = (live[u] & 2) ? comp(tri_v(c, ta[u].y >> 2), ta[u].y & 3) : 0;
+        d[u][2] = (live[u] & 4) ? comp(tri_v(c, ta[u].z >> 2), ta[u].z & 3) : 0;
+    }
+    int2 a[2], b[2], cc[2], p[2][3];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        a[u] = c.P[tv[u].x]; b[u] = c.P[tv[u].y]; cc[u] = c.P[tv[u].z];
+        p[u][0] = c.P[d[u][0]]; p[u][1] = c.P[d[u][1]]; p[u][2] = c.P[d[u][2]];
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        if (ks[u] < 0) continue;
+        if (!on[u]) { c.cand[ks[u]] = make_int2(-1, -1); continue; }   // dropped carried entry
+        int i = -1;
+        if ((live[u] & 1) && incircle_sos(a[u], b[u], cc[u], p[u][0]) > 0) i = 0;
+        else if ((live[u] & 2) && incircle_sos(a[u], b[u], cc[u], p[u][1]) > 0) i = 1;
+        else if ((live[u] & 4) && incircle_sos(a[u], b[u], cc[u], p[u][2]) > 0) i = 2;
+        if (i < 0) { c.cand[ks[u]] = make_int2(-1, -1); continue; }
+        int en = comp(ta[u], i);
+        int n = en >> 2;
+        int key = enc(t[u], i);
+        unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)key));
+        at_max64(&c.claim[t[u]], ck);
+        at_max64(&c.claim[n], ck);
+        c.cand[ks[u]] = make_int2(key, en);
+    }
+}
+
 // Winners flip: t=(A,B,C) with A in slot i, n=(D,C,B) with D in slot j
 // become t=(A,B,D), n=(A,D,C), and both go to the next queue.  Losers are
 // re-queued by body_flip_fix once it is known that nobody flipped them, so
 // every triangle enters the next queue at most once without any
 // de-duplication.
-GCDT_HD void body_flip_do(const Ctx& c, int k) {
-    int2 cd = c.cand[k];
-    if (cd.x < 0) return;
-    int t = cd.x >> 2, i = cd.x & 3;
-    int n = cd.y >> 2, j = cd.y & 3;
-    unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)cd.x));
-    if (c.claim[t] != ck || c.claim[n] != ck) return;
-    int4 tv = tri_v(c, t), ta = tri_a(c, t), nv = tri_v(c, n), na = tri_a(c, n);
+// The flip of claimed candidate (t slot i, n slot j) given both rows, by
+// value (the rows are overwritten here): writes the two new triangles and
+// their flip maps.
+GCDT_HD void do_flip(const Ctx& c, int t, int i, int n, int j,
+                     const int4 tv, const int4 ta, const int4 nv, const int4 na) {
     int i1 = nx3(i), i2 = nx3(i1), j1 = nx3(j), j2 = nx3(j1);
     int A = comp(tv, i), B = comp(tv, i1), C = comp(tv, i2), D = comp(nv, j);
     int ft = tv.w, fn = nv.w;
@@ -686,6 +740,16 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     setc(mn, j1, enc(t, 0)); setc(mn, j2, enc(n, 0));
     c.fmap[t] = mt;
     c.fmap[n] = mn;
+}
+
+GCDT_HD void body_flip_do(const Ctx& c, int k) {
+    int2 cd = c.cand[k];
+    if (cd.x < 0) return;
+    int t = cd.x >> 2, i = cd.x & 3;
+    int n = cd.y >> 2, j = cd.y & 3;
+    unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)cd.x));
+    if (c.claim[t] != ck || c.claim[n] != ck) return;
+    do_flip(c, t, i, n, j, tri_v(c, t), tri_a(c, t), tri_v(c, n), tri_a(c, n));
     // The new diagonal AD is locally Delaunay: queue the four outer edges.
     // Flip number f of the sub-round owns entries 2f, 2f+1 of the next
     // queue; body_flip_fix reads the pairs from there and appends the
@@ -725,6 +789,70 @@ GCDT_HD void body_flip_fix(const Ctx& c, int k) {
     resolve_flip_edge(c, t, 2);
     resolve_flip_edge(c, n, 0);
     resolve_flip_edge(c, n, 1);
+}
+
+// The edge in slot s of flipped triangle tt named the old neighbour `old`
+// (fm = fmap of that neighbour): the write resolve_flip_edge would make.
+GCDT_HD void resolve_flip_loaded(const Ctx& c, int tt, int s, int old, const int4& fm) {
+    if (old < 0) return;
+    int m = old >> 2, ms = old & 3;
+    if (fm.w == (int)c.sr) ((int*)&tri_a(c, tt))[s] = comp(fm, ms);
+    else ((int*)&tri_a(c, m))[ms] = enc(tt, s);
+}
+
+// Two items per thread (k1 < 0: only k0), as body_flip_fix on each, with
+// every stage's loads issued for both items first.
+GCDT_HD void body_flip_fix_pair(const Ctx& c, int k0, int k1) {
+    const int ks[2] = {k0, k1};
+    const int4 none = make_int4(-1, -1, -1, -1);
+    int kind[2], t[2];          // kind 0: nothing, 1: flipped pair, 2: candidate of the queue
+    int2 cd[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        kind[u] = ks[u] < 0 ? 0 : (ks[u] >= c.list_n ? 2 : 1);
+        cd[u] = kind[u] == 2 ? c.cand[ks[u] - c.list_n] : make_int2(-1, -1);
+        t[u] = kind[u] == 1 ? qtri(c.queue_next[2 * ks[u]]) : 0;
+    }
+    int4 ta[2], fl[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        ta[u] = kind[u] == 1 ? tri_a(c, t[u]) : none;
+        fl[u] = (kind[u] == 2 && cd[u].x >= 0) ? c.fmap[cd[u].x >> 2] : none;
+    }
+    // re-queue the candidates that did not flip and whose triangle nobody flipped
+    int rq[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) rq[u] = (kind[u] == 2 && cd[u].x >= 0 && fl[u].w != (int)c.sr) ? 1 : 0;
+    if (rq[0] | rq[1]) {
+        int at = 2 * c.list_n + append_slots(&c.cnt->cur_q, c.base_q, rq[0] + rq[1]);
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+            if (rq[u]) c.queue_next[at++] = c.queue[ks[u] - c.list_n];
+    }
+    // flipped pairs: t's outer edges 0, 2 and n's outer edges 0, 1
+    int n[2];
+    int4 na[2], f0[2], f2[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        n[u] = ta[u].y >> 2;
+        na[u] = kind[u] == 1 ? tri_a(c, n[u]) : none;
+        f0[u] = (kind[u] == 1 && ta[u].x >= 0) ? c.fmap[ta[u].x >> 2] : none;
+        f2[u] = (kind[u] == 1 && ta[u].z >= 0) ? c.fmap[ta[u].z >> 2] : none;
+    }
+    int4 g0[2], g1[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        g0[u] = (kind[u] == 1 && na[u].x >= 0) ? c.fmap[na[u].x >> 2] : none;
+        g1[u] = (kind[u] == 1 && na[u].y >= 0) ? c.fmap[na[u].y >> 2] : none;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        if (kind[u] != 1) continue;
+        resolve_flip_loaded(c, t[u], 0, ta[u].x, f0[u]);
+        resolve_flip_loaded(c, t[u], 2, ta[u].z, f2[u]);
+        resolve_flip_loaded(c, n[u], 0, na[u].x, g0[u]);
+        resolve_flip_loaded(c, n[u], 1, na[u].y, g1[u]);
+    }
 }
 
 // ---------------------------------------------------------------- constraints
