@@ -77,6 +77,9 @@ struct GridExec {
             if (k == K_FLIP_CHECK) {
                 for (; i < count; i += 2 * stride)
                     body_flip_check_pair(c, (int)i, i + stride < count ? (int)(i + stride) : -1);
+            } else if (k == K_FLIP_DO) {
+                for (; i < count; i += 2 * stride)
+                    body_flip_do_pair(c, (int)i, i + stride < count ? (int)(i + stride) : -1);
             } else if (k == K_FLIP_FIX) {
                 for (; i < count; i += 2 * stride)
                     body_flip_fix_pair(c, (int)i, i + stride < count ? (int)(i + stride) : -1);

@@ -499,11 +499,7 @@ GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
 // Winners split their triangle(s).  Child j of a split triangle is the
 // triangle with vertex j replaced by q; it keeps the old edge j in slot j.
 // Outer adjacency is written as the old neighbour and resolved in body_fix.
-GCDT_HD void body_split(const Ctx& c, int k) {
-    int q = c.act[k];
-    int t = c.loc[q];
-    unsigned long long key = ((unsigned long long)c.round << 32) | (0xffffffffu - hash32((uint32_t)q));
-    if (c.vote[t] != key) return;
+GCDT_HD void split_winner(const Ctx& c, int q, int t, unsigned long long key) {
     int e = c.pedge[q];
     int T1 = 2 + 2 * q, T2 = 3 + 2 * q;
     int4 tv = tri_v(c, t), ta = tri_a(c, t);
@@ -556,6 +552,14 @@ GCDT_HD void body_split(const Ctx& c, int k) {
     }
     c.loc[q] = -1;
     c.winners[append_slot(&c.cnt->cur_win, c.base_win)] = make_int2(q, t);
+}
+
+GCDT_HD void body_split(const Ctx& c, int k) {
+    int q = c.act[k];
+    int t = c.loc[q];
+    unsigned long long key = ((unsigned long long)c.round << 32) | (0xffffffffu - hash32((uint32_t)q));
+    if (c.vote[t] != key) return;
+    split_winner(c, q, t, key);
 }
 
 // Child of triangle m (split this round) that now holds m's old edge `ms`.
@@ -757,6 +761,36 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
     int* qn = c.queue_next + 2 * append_slot(&c.cnt->cur_flip, c.base_flip);
     qn[0] = qentry(t, 5);    // (A,B,D): BD and AB
     qn[1] = qentry(n, 3);    // (A,D,C): DC and CA
+}
+
+// Two candidates per thread (k1 < 0: only k0): the candidate and claim
+// loads of both are in flight together; the winners (a minority) then
+// flip one at a time, so only one pair of rows is live at once.
+GCDT_HD void body_flip_do_pair(const Ctx& c, int k0, int k1) {
+    const int ks[2] = {k0, k1};
+    int2 cd[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) cd[u] = ks[u] >= 0 ? c.cand[ks[u]] : make_int2(-1, -1);
+    bool win[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        unsigned long long ck = ((unsigned long long)c.sr << 32) | (0xffffffffu - hash32((uint32_t)cd[u].x));
+        unsigned long long c0 = cd[u].x >= 0 ? c.claim[cd[u].x >> 2] : 0ull;
+        unsigned long long c1 = cd[u].x >= 0 ? c.claim[cd[u].y >> 2] : 0ull;
+        win[u] = cd[u].x >= 0 && c0 == ck && c1 == ck;
+    }
+    const int nw = (int)win[0] + (int)win[1];
+    if (nw == 0) return;
+    int f = append_slots(&c.cnt->cur_flip, c.base_flip, nw);
+#pragma unroll 1
+    for (int u = 0; u < 2; ++u) {
+        if (!win[u]) continue;
+        int t = cd[u].x >> 2, n = cd[u].y >> 2;
+        do_flip(c, t, cd[u].x & 3, n, cd[u].y & 3, tri_v(c, t), tri_a(c, t), tri_v(c, n), tri_a(c, n));
+        int* qn = c.queue_next + 2 * f++;
+        qn[0] = qentry(t, 5);
+        qn[1] = qentry(n, 3);
+    }
 }
 
 GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
