@@ -41,9 +41,9 @@ WORKLOAD = "plain CDT at scale: 10M Gaussian-mixture/uniform int32 points in [1,
 CPU_SAMPLE_POINTS = 2_000_000   # config-shaped sample for the CPU legs (18x18 polygon grid, 632 polygons)
 # DRAM bytes (read + write) of the stage kernel per point, from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the same workload shape at
-# 1,020,608 points: 1,861,193,984 + 903,404,544 bytes.  Reported per solve as
+# 1,020,608 points: 1,890,871,040 + 921,974,272 bytes.  Reported per solve as
 # this figure times N (the full-size capture would replay a 2.9 GB arena ~40x).
-DRAM_BYTES_PER_POINT = (1861193984 + 903404544) / 1020608
+DRAM_BYTES_PER_POINT = (1890871040 + 921974272) / 1020608
 
 
 def rank_info():
