@@ -1,0 +1,157 @@
+// host_emulation.cu -- test harness: the solver's kernel bodies and stage
+// driver compiled for the host and run sequentially, one body call per item,
+// in a chosen item order.  The GPU runs the same bodies in parallel; running
+// them forward, reversed and shuffled on the host checks that a phase's
+// result does not depend on the order its items run in, and the paired
+// bodies (two items per call) are checked against the one-item bodies.
+// Built by tests/test_host_emulation.py into tests/_bin/libhostemu.so.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <random>
+#include <vector>
+#pragma nv_diag_suppress 20011
+#pragma nv_diag_suppress 20014
+#include "../gcdt_b200/csrc/solver.cuh"
+
+using namespace gcdt;
+
+namespace {
+
+int g_order = 0;          // 0 forward, 1 reversed, 2 shuffled
+bool g_pairs = false;     // paired bodies for the passes the GPU runs paired
+bool g_check = false;     // mesh consistency after every split fix and flip fix
+int g_bad = 0;
+std::mt19937 g_rng(1);
+
+// Every live triangle CCW, every adjacency mutual.
+void check_mesh(int kind, const Ctx& c) {
+    if (g_bad) return;
+    for (int t = 0; t < c.ntri; ++t) {
+        bool live = t < 2 || c.loc[(t - 2) / 2] == -1;
+        if (!live) continue;
+        int4 v = tri_v(c, t), a = tri_a(c, t);
+        if (orient2d(c.P[v.x], c.P[v.y], c.P[v.z]) <= 0) { g_bad = 100 + kind; return; }
+        for (int s = 0; s < 3; ++s) {
+            int en = comp(a, s);
+            if (en < 0) continue;
+            if (comp(tri_a(c, en >> 2), en & 3) != ((t << 2) | s)) { g_bad = 200 + kind; return; }
+        }
+    }
+}
+
+void host_phase(int k, const Ctx& c, long long n) {
+    std::vector<int> idx((size_t)n);
+    std::iota(idx.begin(), idx.end(), 0);
+    if (g_order == 1) std::reverse(idx.begin(), idx.end());
+    if (g_order == 2) std::shuffle(idx.begin(), idx.end(), g_rng);
+    if (g_pairs && (k == K_FLIP_CHECK || k == K_FLIP_DO || k == K_FLIP_FIX)) {
+        for (size_t m = 0; m < idx.size(); m += 2) {
+            int k1 = m + 1 < idx.size() ? idx[m + 1] : -1;
+            if (k == K_FLIP_CHECK) body_flip_check_pair(c, idx[m], k1);
+            else if (k == K_FLIP_DO) body_flip_do_pair(c, idx[m], k1);
+            else body_flip_fix_pair(c, idx[m], k1);
+        }
+    } else {
+        for (int i : idx) dispatch(k, c, i);
+    }
+    if (g_check && (k == K_FIX || k == K_FLIP_FIX)) check_mesh(k, c);
+}
+
+// One block's executor: no single-block hand-off.
+struct HostBlock {
+    static constexpr bool kCanNarrow = false;
+    Counters* cnt;
+    void phase(int k, const Ctx& c, long long n) { host_phase(k, c, n); }
+    unsigned long long cursor(unsigned long long* p) { return *p; }
+    int word(int* p) { return *p; }
+    int narrow_flips(Ctx&, Driver&, long long&) { return ST_INTERNAL; }
+    int narrow_rounds(Ctx&, Driver&, long long) { return ST_INTERNAL; }
+    void finish(const Ctx&, long long, long long, long long, int) {}
+};
+
+// The whole grid's executor, with the single-block tails run as HostBlock.
+struct HostGrid {
+    static constexpr bool kCanNarrow = true;
+    Counters* cnt;
+    int narrow_flips(Ctx& c, Driver& D, long long& nq) {
+        HostBlock bx{cnt};
+        Driver Db = D;
+        Ctx cb = c;
+        long long left = nq;
+        int rc = flip_loop(bx, cb, Db, left, 4 * kNarrowQueue);
+        D = Db;
+        nq = left;
+        return rc;
+    }
+    int narrow_rounds(Ctx& c, Driver& D, long long nact) {
+        HostBlock bx{cnt};
+        Driver Db = D;
+        Ctx cb = c;
+        int rc = insert_rounds(bx, cb, Db, nact);
+        D = Db;
+        return rc;
+    }
+    void phase(int k, const Ctx& c, long long n) { host_phase(k, c, n); }
+    unsigned long long cursor(unsigned long long* p) { return *p; }
+    int word(int* p) { return *p; }
+    void finish(const Ctx&, long long r, long long s, long long cr, int rc) {
+        cnt->rounds = r;
+        cnt->flip_subrounds = s;
+        cnt->constraint_rounds = cr;
+        cnt->status |= rc;
+    }
+};
+
+struct HostBackend {
+    Counters* cnt;
+    void launch(int k, const Ctx& c, long long n) { host_phase(k, c, n); }
+    void fill(void* p, int v, size_t b) { std::memset(p, v, b); }
+    void read(Counters* h) { *h = *cnt; }
+    void stages(const Ctx& c0) {
+        Ctx c = c0;
+        HostGrid ex{cnt};
+        run_stages(ex, c);
+    }
+    void sort(Ctx& c, int n) {
+        std::vector<std::pair<unsigned long long, int>> v(n);
+        for (int i = 0; i < n; ++i) v[i] = {c.keys[i], c.vals[i]};
+        std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (int i = 0; i < n; ++i) { c.keys[i] = v[i].first; c.vals[i] = v[i].second; }
+    }
+};
+
+}  // namespace
+
+// Solve on the host.  order: 0 forward, 1 reversed, 2 shuffled (seeded);
+// pairs: use the paired flip bodies; check: mesh check after each fix phase.
+// stats[0..4] = status, insertion rounds, flip sub-rounds, flips, constraint
+// rounds; returns the status bits, or 1000+ when the mesh check failed.
+extern "C" int host_triangulate(const int* xy, int n, const int* cons, int s, int* tris, int* adj,
+                                unsigned char* cflags, long long* stats, int order, int pairs, int check) {
+    g_order = order;
+    g_pairs = pairs != 0;
+    g_check = check != 0;
+    g_bad = 0;
+    g_rng.seed(12345);
+    Plan p = make_plan(n, s, 0);
+    std::vector<char> arena(p.L.total + 256);
+    char* base = (char*)(((uintptr_t)arena.data() + 255) & ~(uintptr_t)255);
+    Ctx c = bind_ctx(base, p);
+    c.in_xy = (const int2*)xy;
+    c.in_cons = (const int2*)cons;
+    c.out_tris = tris;
+    c.out_adj = adj;
+    c.out_cflags = cflags;
+    HostBackend bk{c.cnt};
+    SolveStats ss;
+    int rc = run_solve(bk, c, ss);
+    stats[0] = rc;
+    stats[1] = ss.rounds;
+    stats[2] = ss.flip_subrounds;
+    stats[3] = ss.flips;
+    stats[4] = ss.constraint_rounds;
+    return g_bad ? 1000 + g_bad : rc;
+}
