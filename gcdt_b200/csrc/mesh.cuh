@@ -669,42 +669,42 @@ GCDT_HD void body_flip_check(const Ctx& c, int k) {
 // for both entries before either is used: twice the loads in flight per
 // thread for this latency-bound pass.  Same result as body_flip_check on
 // each entry.
-GCDT_HD void body_flip_check_pair(const Ctx& c, int k0, int k1) {
-    const int ks[2] = {k0, k1};
-    bool on[2];
-    int t[2], mask[2];
+template <int W>
+GCDT_HD void flip_check_multi(const Ctx& c, const int (&ks)[W]) {
+    bool on[W];
+    int t[W], mask[W];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < W; ++u) {
         on[u] = ks[u] >= 0;
         int qe = on[u] ? c.queue[ks[u]] : 0;
         t[u] = qtri(qe);
         mask[u] = qe & 7;
     }
 #pragma unroll
-    for (int u = 0; u < 2; ++u)
+    for (int u = 0; u < W; ++u)
         if (on[u] && ks[u] < c.carry_n && c.ins[t[u]].x == (int)c.round) on[u] = false;
-    int4 tv[2], ta[2];
+    int4 tv[W], ta[W];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < W; ++u) {
         tv[u] = on[u] ? tri_v(c, t[u]) : make_int4(0, 0, 0, 7);
         ta[u] = on[u] ? tri_a(c, t[u]) : make_int4(-1, -1, -1, 0);
     }
-    int live[2], d[2][3];
+    int live[W], d[W][3];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < W; ++u) {
         live[u] = mask[u] & ~tv[u].w & ((ta[u].x >= 0) | ((ta[u].y >= 0) << 1) | ((ta[u].z >= 0) << 2));
         d[u][0] = (live[u] & 1) ? comp(tri_v(c, ta[u].x >> 2), ta[u].x & 3) : 0;
         d[u][1] = (live[u] & 2) ? comp(tri_v(c, ta[u].y >> 2), ta[u].y & 3) : 0;
         d[u][2] = (live[u] & 4) ? comp(tri_v(c, ta[u].z >> 2), ta[u].z & 3) : 0;
     }
-    int2 a[2], b[2], cc[2], p[2][3];
+    int2 a[W], b[W], cc[W], p[W][3];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < W; ++u) {
         a[u] = c.P[tv[u].x]; b[u] = c.P[tv[u].y]; cc[u] = c.P[tv[u].z];
         p[u][0] = c.P[d[u][0]]; p[u][1] = c.P[d[u][1]]; p[u][2] = c.P[d[u][2]];
     }
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < W; ++u) {
         if (ks[u] < 0) continue;
         if (!on[u]) { c.cand[ks[u]] = make_int2(-1, -1); continue; }   // dropped carried entry
         int i = -1;
@@ -720,6 +720,11 @@ GCDT_HD void body_flip_check_pair(const Ctx& c, int k0, int k1) {
         at_max64(&c.claim[n], ck);
         c.cand[ks[u]] = make_int2(key, en);
     }
+}
+
+GCDT_HD void body_flip_check_pair(const Ctx& c, int k0, int k1) {
+    const int ks[2] = {k0, k1};
+    flip_check_multi<2>(c, ks);
 }
 
 // Winners flip: t=(A,B,C) with A in slot i, n=(D,C,B) with D in slot j

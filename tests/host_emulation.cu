@@ -21,7 +21,7 @@ using namespace gcdt;
 namespace {
 
 int g_order = 0;          // 0 forward, 1 reversed, 2 shuffled
-bool g_pairs = false;     // paired bodies for the passes the GPU runs paired
+int g_width = 1;          // items per call in the flip passes (1: one-item bodies)
 bool g_check = false;     // mesh consistency after every split fix and flip fix
 int g_bad = 0;
 std::mt19937 g_rng(1);
@@ -47,12 +47,16 @@ void host_phase(int k, const Ctx& c, long long n) {
     std::iota(idx.begin(), idx.end(), 0);
     if (g_order == 1) std::reverse(idx.begin(), idx.end());
     if (g_order == 2) std::shuffle(idx.begin(), idx.end(), g_rng);
-    if (g_pairs && (k == K_FLIP_CHECK || k == K_FLIP_DO || k == K_FLIP_FIX)) {
-        for (size_t m = 0; m < idx.size(); m += 2) {
-            int k1 = m + 1 < idx.size() ? idx[m + 1] : -1;
-            if (k == K_FLIP_CHECK) body_flip_check_pair(c, idx[m], k1);
-            else if (k == K_FLIP_DO) body_flip_do_pair(c, idx[m], k1);
-            else body_flip_fix_pair(c, idx[m], k1);
+    if (g_width > 1 && (k == K_FLIP_CHECK || k == K_FLIP_DO || k == K_FLIP_FIX)) {
+        const size_t w = k == K_FLIP_CHECK ? (size_t)g_width : 2;
+        for (size_t m = 0; m < idx.size(); m += w) {
+            int ks[4];
+            for (size_t u = 0; u < 4; ++u) ks[u] = m + u < idx.size() && u < w ? idx[m + u] : -1;
+            if (k == K_FLIP_CHECK && w == 2) body_flip_check_pair(c, ks[0], ks[1]);
+            else if (k == K_FLIP_CHECK && w == 3) { const int k3[3] = {ks[0], ks[1], ks[2]}; flip_check_multi<3>(c, k3); }
+            else if (k == K_FLIP_CHECK) { const int k4[4] = {ks[0], ks[1], ks[2], ks[3]}; flip_check_multi<4>(c, k4); }
+            else if (k == K_FLIP_DO) body_flip_do_pair(c, ks[0], ks[1]);
+            else body_flip_fix_pair(c, ks[0], ks[1]);
         }
     } else {
         for (int i : idx) dispatch(k, c, i);
@@ -126,13 +130,15 @@ struct HostBackend {
 }  // namespace
 
 // Solve on the host.  order: 0 forward, 1 reversed, 2 shuffled (seeded);
-// pairs: use the paired flip bodies; check: mesh check after each fix phase.
+// width: items per call in the flip passes (1: one-item bodies, 2: the
+// paired bodies the GPU uses, 3-4: wider flip checks); check: mesh check
+// after each fix phase.
 // stats[0..4] = status, insertion rounds, flip sub-rounds, flips, constraint
 // rounds; returns the status bits, or 1000+ when the mesh check failed.
 extern "C" int host_triangulate(const int* xy, int n, const int* cons, int s, int* tris, int* adj,
-                                unsigned char* cflags, long long* stats, int order, int pairs, int check) {
+                                unsigned char* cflags, long long* stats, int order, int width, int check) {
     g_order = order;
-    g_pairs = pairs != 0;
+    g_width = width < 1 ? 1 : (width > 4 ? 4 : width);
     g_check = check != 0;
     g_bad = 0;
     g_rng.seed(12345);

@@ -41,7 +41,7 @@ def emu():
     L.host_triangulate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, i32, i32, i32]
     L.host_triangulate.restype = i32
 
-    def run(xy, cons, order=0, pairs=False, check=True):
+    def run(xy, cons, order=0, width=1, check=True):
         xy = np.ascontiguousarray(xy, np.int32)
         cons = np.ascontiguousarray(cons, np.int32).reshape(-1, 2)
         n, s, T = len(xy), len(cons), 2 * len(xy) + 2
@@ -50,7 +50,7 @@ def emu():
         cf = np.zeros(T, np.uint8)
         st = np.zeros(8, np.int64)
         p = lambda a: ctypes.c_void_p(a.ctypes.data)
-        rc = L.host_triangulate(p(xy), n, p(cons), s, p(tris), p(adj), p(cf), p(st), order, int(pairs), int(check))
+        rc = L.host_triangulate(p(xy), n, p(cons), s, p(tris), p(adj), p(cf), p(st), order, int(width), int(check))
         return rc, tris, adj, cf, st
     return run
 
@@ -72,7 +72,7 @@ def _cases():
 
 @pytest.mark.parametrize("name,xy,cons", _cases(), ids=[c[0] for c in _cases()])
 def test_host_emulation_matches_oracle_in_every_order(emu, name, xy, cons):
-    runs = [emu(xy, cons, order, pairs) for order in (0, 1, 2) for pairs in (False, True)]
+    runs = [emu(xy, cons, order, width) for order in (0, 1, 2) for width in (1, 2)]
     for rc, *_ in runs:
         assert rc == 0, "status %d (1000+: mesh check failed)" % rc
     ref = runs[0]
