@@ -51,6 +51,63 @@ def rank_info():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+# ---- replicas: N > 1 runs one independent solve per rank (the path has no
+# data exchange); ranks only meet for barriers and the timing reductions.
+
+def dist_init(backend):
+    """Join the torchrun process group (no-op for one rank); returns
+    (rank, world, local_rank)."""
+    import datetime
+    import torch.distributed as dist
+    rank, world, local = rank_info()
+    if world > 1:
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def dist_done(world):
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _reduce(x, world, device, op):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
+def max_over_ranks(x, world, device):
+    """The slowest rank's time: the job's time."""
+    import torch.distributed as dist
+    return _reduce(x, world, device, dist.ReduceOp.MAX)
+
+
+def sum_over_ranks(x, world, device):
+    import torch.distributed as dist
+    return _reduce(x, world, device, dist.ReduceOp.SUM)
+
+
+def replica_workload(rank, scale_points=0):
+    """Rank r's own seeded instance of the scale workload (seed 1 + r); with
+    scale_points, a reduced copy of the same shape (profiling and tests)."""
+    import gcdt_b200 as g
+    if scale_points:
+        gsz = max(2, int(round(56 * (scale_points / 10_000_000) ** 0.5)))
+        return g.generate(g.GEN_SCALE, 1 + rank, scale_points, gsz, int(gsz * gsz * 3125 / 3136))
+    return g.generate(g.GEN_SCALE, 1 + rank)
+
+
+def job_mpts(total_points, ms):
+    """Whole-job throughput: the points of all ranks over the slowest rank's time."""
+    return total_points / (ms * 1e-3) / 1e6
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -156,19 +213,12 @@ def run_ours(args):
     import torch.distributed as dist
     import gcdt_b200 as g
 
-    rank, world, local = rank_info()
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    rank, world, local = dist_init("nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
     # replicas: rank r triangulates its own seeded instance of the workload
-    if args.scale_points:
-        # reduced copy of the workload shape, for profiling runs only
-        gsz = max(2, int(round(56 * (args.scale_points / 10_000_000) ** 0.5)))
-        xy, cons = g.generate(g.GEN_SCALE, 1 + rank, args.scale_points, gsz, int(gsz * gsz * 3125 / 3136))
-    else:
-        xy, cons = g.generate(g.GEN_SCALE, 1 + rank)
+    xy, cons = replica_workload(rank, args.scale_points)
     n, s = len(xy), len(cons)
     tri = g.Triangulator(max_points=n, max_segments=s, device=local)
     stream = torch.cuda.current_stream(dev)
@@ -186,12 +236,7 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    total_points = sum_over_ranks(float(n), world, dev)
 
     # ---- device-resident timing
     for _ in range(args.warmup):
@@ -212,8 +257,8 @@ def run_ours(args):
     prof = tri.phase_profile()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ms_local = statistics.median(step_ms)
-    ms = max_over_ranks(ms_local)
-    value = world * n / (ms * 1e-3) / 1e6
+    ms = max_over_ranks(ms_local, world, dev)
+    value = job_mpts(total_points, ms)
     st = tri.stats()
 
     # ---- end-to-end through the public API from pinned host memory
@@ -238,7 +283,7 @@ def run_ours(args):
         b.synchronize()
         if k >= args.warmup:
             e2e_ms.append(a.elapsed_time(b))
-    e2e_serial = max_over_ranks(statistics.median(e2e_ms))
+    e2e_serial = max_over_ranks(statistics.median(e2e_ms), world, dev)
     # (b) a stream of inputs, double-buffered: two contexts on two streams
     # with the asynchronous entry point, the solves ordered by events (each
     # solve's persistent kernel holds the whole GPU), so step k's input and
@@ -277,7 +322,7 @@ def run_ours(args):
     t_end.synchronize()
     for t in ctxs:
         t.wait()                        # raises if any solve failed
-    e2e = max_over_ranks(t_start.elapsed_time(t_end) / args.steps)
+    e2e = max_over_ranks(t_start.elapsed_time(t_end) / args.steps, world, dev)
     tri2.close()
     h2d = xy.nbytes + cons.nbytes
     d2h = T * 12 * 2 + T
@@ -317,11 +362,11 @@ def run_ours(args):
                          "unit_of_work": "one full solve; algorithmic bytes 8N+8S+25(2N+2) = %d" % b_alg,
                          "peak_source": peak_kind},
             "cpu_baseline": cpu,
-            "e2e": {"value": world * n / (e2e * 1e-3) / 1e6, "unit": UNIT,
+            "e2e": {"value": job_mpts(total_points, e2e), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e,
                     "mode": "stream of inputs, double-buffered on two streams (solves serialized, "
                             "copies overlapped)",
-                    "serial": {"value": world * n / (e2e_serial * 1e-3) / 1e6, "ms_per_step": e2e_serial,
+                    "serial": {"value": job_mpts(total_points, e2e_serial), "ms_per_step": e2e_serial,
                                "mode": "one step at a time (copy in, solve, copy out, wait)"}},
             "gpu_launches": launches,
             "clocks": clocks,
@@ -333,9 +378,7 @@ def run_ours(args):
         }
         print(json.dumps(line), flush=True)
     tri.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    dist_done(world)
 
 
 def run_batched(args):
