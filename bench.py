@@ -17,9 +17,10 @@ the one-step-at-a-time figure.
 N > 1 runs independent replicas, one per rank (the path has no data-parallel
 exchange: a single triangulation stays on one GPU), so scaling is weak.
 
---impl reference times the CPU path (the single-threaded exact oracle, the
-reference having no host implementation of this path) on bounded samples of
-the same workload shape.
+--impl reference times the CPU path (the sequential exact oracle, the
+reference having no host implementation of this path) on every host thread
+at once, each thread solving its own bounded sample of the same workload
+shape.
 """
 import argparse
 import json
@@ -183,16 +184,57 @@ def cpu_oracle_sample(seed=1, repeat=1):
     return len(xy) / t / 1e6, sample, len(xy), t
 
 
+# Peak resident bytes of one oracle solve of the CPU sample (its 2.02M points,
+# the mesh, the Morton keys and the outputs measured at ~210 MB), with margin.
+CPU_SAMPLE_BYTES = 400 << 20
+
+
+def cpu_threads():
+    """Host threads for the CPU leg: every core this process may run on,
+    fewer if half the available memory cannot hold one sample per thread."""
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        with open("/proc/meminfo") as f:
+            avail = next(int(l.split()[1]) * 1024 for l in f if l.startswith("MemAvailable:"))
+        cores = min(cores, max(1, avail // 2 // CPU_SAMPLE_BYTES))
+    except Exception:
+        pass
+    return max(1, cores)
+
+
+def cpu_oracle_parallel(threads, steps, points=CPU_SAMPLE_POINTS):
+    """Time the sequential oracle on every host thread at once, each thread
+    solving its own seeded config-shaped sample; one step = all threads'
+    solves, timed from the common start to the last finish.  Returns the
+    per-step (Mpts/s, seconds) and the sample description."""
+    from concurrent.futures import ThreadPoolExecutor
+    import gcdt_b200 as g
+    from oracle import oracle
+    with ThreadPoolExecutor(threads) as ex:
+        samples = list(ex.map(lambda i: g.generate(g.GEN_SCALE, 1 + i, points, 18, 316),
+                              range(threads)))
+        total = sum(len(xy) for xy, _ in samples)
+        out = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            rcs = list(ex.map(lambda s: oracle.cdt(*s)[0], samples))
+            t = time.perf_counter() - t0
+            if any(rcs):
+                raise RuntimeError("oracle failed on a CPU sample: %r" % (rcs,))
+            out.append((total / t / 1e6, t))
+    desc = ("%d concurrent samples (one per thread) of ~%d points + %d segments each, %d points in all "
+            "(scale workload shape, 18x18 polygon grid, seeds 1..%d)" % (
+                threads, len(samples[0][0]), len(samples[0][1]), total, threads))
+    return out, desc
+
+
 def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
         return
-    vals = []
-    sample = None
-    for i in range(args.warmup + args.steps):
-        v, sample, n, t = cpu_oracle_sample(seed=1 + i)
-        if i >= args.warmup:
-            vals.append((v, t))
+    threads = cpu_threads()
+    runs, sample = cpu_oracle_parallel(threads, args.warmup + args.steps)
+    vals = runs[args.warmup:]
     value = statistics.median([v for v, _ in vals])
     ms = statistics.median([t for _, t in vals]) * 1e3
     line = {
@@ -200,9 +242,11 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "i64/i128 exact predicates on i32 coordinates", "data": "synthetic",
-        "config": {"workload": WORKLOAD + " -- CPU leg: bounded sample per step", "parallelism": "none (1 core)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": sample + "; single-threaded exact incremental CDT (oracle/cdt_oracle.c); the reference has no host implementation of this path"},
+        "config": {"workload": WORKLOAD + " -- CPU leg: bounded samples per step",
+                   "parallelism": "%d host threads, one independent sample each" % threads},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample + "; sequential exact incremental CDT (oracle/cdt_oracle.c) per thread; "
+                                   "the reference has no host implementation of this path"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

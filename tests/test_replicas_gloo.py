@@ -65,3 +65,15 @@ def test_replica_workloads_are_seeded_per_rank():
     a1, _ = bench.replica_workload(1, scale_points=20000)
     assert np.array_equal(a0, b0) and np.array_equal(c0, d0)
     assert not np.array_equal(a0[:1000], a1[:1000])
+
+
+def test_reference_arm_runs_one_sample_per_thread():
+    """The --impl reference leg: every thread solves its own seeded sample,
+    all of them complete, and the step figure is all points over the step."""
+    import bench
+    runs, desc = bench.cpu_oracle_parallel(2, 2, points=30000)
+    assert len(runs) == 2 and desc.startswith("2 concurrent samples")
+    total = int(desc.split(" points in all")[0].rsplit(" ", 1)[1])
+    for v, t in runs:
+        assert t > 0 and abs(v - total / t / 1e6) < 1e-9
+    assert 1 <= bench.cpu_threads() <= (os.cpu_count() or 1)
