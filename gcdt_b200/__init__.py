@@ -130,6 +130,10 @@ def lib():
     L.gcdt_text_save.restype = ctypes.c_int
     L.gcdt_eval_predicates.argtypes = [vp, i32, vp, vp]
     L.gcdt_eval_predicates.restype = ctypes.c_int
+    L.gcdt_reference_layout_scratch_bytes.argtypes = [i32, i32]
+    L.gcdt_reference_layout_scratch_bytes.restype = ctypes.c_size_t
+    L.gcdt_reference_layout.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
+    L.gcdt_reference_layout.restype = ctypes.c_int
     _LIB = L
     return L
 
@@ -329,6 +333,41 @@ def eval_predicates(quads):
     if rc != 0:
         raise GcdtError(rc, "gcdt_eval_predicates")
     return out.cpu().numpy()
+
+
+def reference_layout(points, tris, adj=None, cflags=None, stream=None):
+    """The mesh in the reference's output layout (delaunayNew's Morton
+    renumbering, yingtix/gCDT kernel.cu:1886-2068), on the device.
+
+    points: (n, 2) int32 CUDA tensor (the caller's points, corners implied);
+    tris/adj: (T, 3) int32 and cflags: (T,) uint8 CUDA tensors over vertices
+    0..n+3, e.g. Triangulator.triangulate's output.  Returns (points (n+4, 2)
+    in Morton order, labels (n+4,) = new number of each vertex, tris, adj or
+    None, cflags or None), all sorted as gcdt_reference_layout describes."""
+    import torch
+    n = int(points.shape[0])
+    T = int(tris.shape[0])
+    dev = tris.device if T else points.device
+    for t in (points, tris, adj, cflags):
+        if t is not None and (not t.is_cuda or not t.is_contiguous()):
+            raise ValueError("reference_layout takes contiguous CUDA tensors")
+    pts_out = torch.empty((n + 4, 2), dtype=torch.int32, device=dev)
+    labels = torch.empty((n + 4,), dtype=torch.int32, device=dev)
+    tris_out = torch.empty((T, 3), dtype=torch.int32, device=dev)
+    adj_out = torch.empty((T, 3), dtype=torch.int32, device=dev) if adj is not None else None
+    cf_out = torch.empty((T,), dtype=torch.uint8, device=dev) if cflags is not None else None
+    need = int(lib().gcdt_reference_layout_scratch_bytes(n, T))
+    scratch = torch.empty((max(need, 256),), dtype=torch.uint8, device=dev)
+    if stream is None:
+        stream = torch.cuda.current_stream(dev).cuda_stream
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None and t.numel() else 0)
+    with torch.cuda.device(dev):
+        rc = lib().gcdt_reference_layout(ptr(points), n, ptr(tris), ptr(adj), ptr(cflags), T,
+                                         ptr(pts_out), ptr(labels), ptr(tris_out), ptr(adj_out), ptr(cf_out),
+                                         ptr(scratch), scratch.numel(), ctypes.c_void_p(stream))
+    if rc != 0:
+        raise GcdtError(rc, "gcdt_reference_layout")
+    return pts_out, labels, tris_out, adj_out, cf_out
 
 
 class BatchConfig(ctypes.Structure):

@@ -120,6 +120,40 @@ const char* gcdt_phase_name(int32_t kind);
    inCircle used by the triangulator. */
 gcdt_status gcdt_eval_predicates(const int32_t* d_quads, int32_t n_cases, int32_t* d_out, void* stream);
 
+/* ---- The reference's output layout.  yingtix/gCDT returns its mesh in
+   Morton order: delaunayNew (kernel.cu:4697-4701) renumbers the n+4 points
+   (corners included) by a stable sort on the 30-bit Morton code of
+   (x >> 15, y >> 15) (reorderPoints, kernel.cu:1966-2068) and sorts the
+   triangles stably by the code of their centroid (mean of the vertices'
+   (x >> 15, y >> 15), integer division; reorderFaces, kernel.cu:1886-1964).
+   This call applies both orders to a triangulation given in input index
+   order (gcdt_triangulate's output, or any mesh over those n+4 vertices):
+     d_points_out  2(n+4) int32: sorted point j = vertex perm[j] (corners
+                   n..n+3 are (0,0), (R,0), (R,R), (0,R)); identical to the
+                   reference's returned point array;
+     d_labels      n+4 int32: new number of vertex i;
+     d_tris_out    triangle j = input triangle order[j], vertices renumbered
+                   (each triangle keeps its own vertex rotation);
+     d_adj_out     neighbours renumbered to their new positions, -1 kept
+                   (with d_adj; NULL together with d_adj);
+     d_cflags_out  flags moved with their triangle (NULL with d_cflags).
+   Ties in the triangle code keep the input triangle order; the reference
+   breaks them by its pre-flip slot order (it sorts before its last flips),
+   so only the point array is expected to equal the reference's byte for
+   byte.  d_scratch (256-byte aligned) holds at least
+   gcdt_reference_layout_scratch_bytes(n, n_tris) bytes; outputs must not
+   overlap inputs, scratch or each other.  Runs on the current device and
+   returns when the result is complete on `stream`; GCDT_BAD_INPUT if a
+   vertex id or neighbour id is out of range (those entries become -1),
+   GCDT_OOM if the scratch is too small. */
+size_t gcdt_reference_layout_scratch_bytes(int32_t n_points, int32_t n_tris);
+gcdt_status gcdt_reference_layout(const int32_t* d_points, int32_t n,
+                                  const int32_t* d_tris, const int32_t* d_adj,
+                                  const uint8_t* d_cflags, int32_t n_tris,
+                                  int32_t* d_points_out, int32_t* d_labels,
+                                  int32_t* d_tris_out, int32_t* d_adj_out, uint8_t* d_cflags_out,
+                                  void* d_scratch, size_t scratch_bytes, void* stream);
+
 /* ---- Batched triangulation (no counterpart in the reference, which
    triangulates one point set per process, kernel.cu:5332-5466).
    Many independent instances in one launch: one segmented Morton sort,

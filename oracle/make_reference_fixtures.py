@@ -5,12 +5,17 @@ oracle/build_ref.sh from the reference sources).  For each seeded input it
 runs the reference's own device pipeline (kernel.cu:5398-5443), maps its
 triangles to input indices by coordinates and records the SHA-256 of the
 canonical triangle set, the triangle count, the reference's final Delaunay
-self-check count (`mark`, kernel.cu:4839-4844) and the number of constraints
-it ignored (`sum ig`, addConstraints.cu:1744-1751).  A case pins parity only
+self-check count (`mark`, kernel.cu:4839-4844), the number of constraints
+it ignored (`sum ig`, addConstraints.cu:1744-1751) and the SHA-256 of the
+point array it returns (Morton-renumbered by reorderPoints,
+kernel.cu:1966-2068; the check for gcdt_reference_layout).  A case pins parity only
 where the reference's output is complete: mark == 0, nothing ignored and
 2n+2 triangles ("pinned": true).
 
-    CUDA_MODULE_LOADING=EAGER python oracle/make_reference_fixtures.py
+    CUDA_MODULE_LOADING=EAGER python oracle/make_reference_fixtures.py [case names]
+
+Named cases are re-run and merged into the existing file; no names re-runs
+every case.
 """
 import hashlib
 import json
@@ -43,9 +48,19 @@ def sha(a):
 
 def main():
     os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
+    path = os.path.join(ROOT, "tests", "golden", "reference_fixtures.json")
+    only = set(sys.argv[1:])
     out = {"reference": "yingtix/gCDT device pipeline, kernel.cu:5398-5443, built by oracle/build_ref.sh",
            "cases": []}
+    old = {}
+    if only and os.path.exists(path):
+        with open(path) as f:
+            old = {c["name"]: c for c in json.load(f)["cases"]}
     for name, kind, seed, args, drop in CASES:
+        if only and name not in only:
+            if name in old:
+                out["cases"].append(old[name])
+            continue
         xy, cons = g.generate(kind, seed, *args)
         if drop:
             cons = cons[:0]
@@ -58,10 +73,10 @@ def main():
                 "ref_ntri": T, "ref_mark": mark, "ref_ignored": ignored, "ref_event_ms": r["event_ms"],
                 "ref_sum_time_ms": r["sum_time"],
                 "pinned": bool(mark == 0 and ignored == 0 and T == 2 * len(xy) + 2),
-                "tris_sha256": sha(g.canonical(r["tris"]))}
+                "tris_sha256": sha(g.canonical(r["tris"])),
+                "points_sha256": sha(r["points"])}
         out["cases"].append(case)
         print(json.dumps(case), flush=True)
-    path = os.path.join(ROOT, "tests", "golden", "reference_fixtures.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", path)

@@ -24,9 +24,10 @@ def available():
 
 
 def run(xy, cons=None, repeat=1, timeout=600):
-    """-> dict(tris (T,3) in input ids with corners n..n+3, event_ms, sum_time,
-    marks [final Delaunay self-check counts], ignored [constraints the
-    reference dropped], stdout)."""
+    """-> dict(tris (T,3) in input ids with corners n..n+3, points (n+4,2) =
+    the reference's returned (Morton-permuted) point array, event_ms,
+    sum_time, marks [final Delaunay self-check counts], ignored [constraints
+    the reference dropped], stdout)."""
     xy = np.ascontiguousarray(xy, dtype=np.int32).reshape(-1, 2)
     cons = np.ascontiguousarray(np.zeros((0, 2)) if cons is None else cons, dtype=np.int32).reshape(-1, 2)
     n, s = len(xy), len(cons)
@@ -62,5 +63,5 @@ def run(xy, cons=None, repeat=1, timeout=600):
     marks = [int(m) for m in re.findall(r"^mark (-?\d+)", out, re.M)]
     ignored = [int(m) for m in re.findall(r"^sum ig: (-?\d+)", out, re.M)]
     reps = [float(m) for m in re.findall(r"^harness rep \d+ event_ms ([0-9.]+)", out, re.M)]
-    return {"tris": mapped, "event_ms": event_ms, "rep_ms": reps, "sum_time": sum_time,
+    return {"tris": mapped, "points": pts.copy(), "event_ms": event_ms, "rep_ms": reps, "sum_time": sum_time,
             "marks": marks, "ignored": ignored, "stdout": out}
