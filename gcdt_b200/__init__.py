@@ -134,6 +134,10 @@ def lib():
     L.gcdt_reference_layout_scratch_bytes.restype = ctypes.c_size_t
     L.gcdt_reference_layout.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
     L.gcdt_reference_layout.restype = ctypes.c_int
+    L.gcdt_classify_regions_scratch_bytes.argtypes = [i32]
+    L.gcdt_classify_regions_scratch_bytes.restype = ctypes.c_size_t
+    L.gcdt_classify_regions.argtypes = [vp, vp, i32, vp, ctypes.POINTER(i32), vp, ctypes.c_size_t, vp]
+    L.gcdt_classify_regions.restype = ctypes.c_int
     _LIB = L
     return L
 
@@ -368,6 +372,33 @@ def reference_layout(points, tris, adj=None, cflags=None, stream=None):
     if rc != 0:
         raise GcdtError(rc, "gcdt_reference_layout")
     return pts_out, labels, tris_out, adj_out, cf_out
+
+
+def classify_regions(adj, cflags, stream=None):
+    """Even-odd region depth of every triangle, on the device.
+
+    adj: (T, 3) int32 and cflags: (T,) uint8 CUDA tensors (a solve's output).
+    Returns (depth (T,) int32 CUDA tensor, greatest depth): depth = fewest
+    constraint edges crossed from the box edge; odd = inside the polygons."""
+    import torch
+    T = int(adj.shape[0])
+    for t in (adj, cflags):
+        if not t.is_cuda or not t.is_contiguous():
+            raise ValueError("classify_regions takes contiguous CUDA tensors")
+    depth = torch.empty((T,), dtype=torch.int32, device=adj.device)
+    need = int(lib().gcdt_classify_regions_scratch_bytes(T))
+    scratch = torch.empty((max(need, 256),), dtype=torch.uint8, device=adj.device)
+    if stream is None:
+        stream = torch.cuda.current_stream(adj.device).cuda_stream
+    md = ctypes.c_int32(0)
+    with torch.cuda.device(adj.device):
+        rc = lib().gcdt_classify_regions(ctypes.c_void_p(adj.data_ptr()), ctypes.c_void_p(cflags.data_ptr()), T,
+                                         ctypes.c_void_p(depth.data_ptr()), ctypes.byref(md),
+                                         ctypes.c_void_p(scratch.data_ptr()), scratch.numel(),
+                                         ctypes.c_void_p(stream))
+    if rc != 0:
+        raise GcdtError(rc, "gcdt_classify_regions")
+    return depth, int(md.value)
 
 
 class BatchConfig(ctypes.Structure):

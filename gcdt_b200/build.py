@@ -58,7 +58,7 @@ def _deps(*names):
 
 def build(force=False, verbose=False, ptxas_verbose=False):
     out = os.path.join(HERE, "libgcdt_b200.so")
-    srcs = ["gcdt.cu", "batch.cu", "server.cu", "surface.cu", "reorder.cu", "io.cpp"]
+    srcs = ["gcdt.cu", "batch.cu", "server.cu", "surface.cu", "reorder.cu", "regions.cu", "io.cpp"]
     if force or _stale(out, _deps(*srcs)):
         flags = list(NVCC_FLAGS)
         if ptxas_verbose:

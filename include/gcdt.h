@@ -154,6 +154,23 @@ gcdt_status gcdt_reference_layout(const int32_t* d_points, int32_t n,
                                   int32_t* d_tris_out, int32_t* d_adj_out, uint8_t* d_cflags_out,
                                   void* d_scratch, size_t scratch_bytes, void* stream);
 
+/* ---- Inside / outside (no counterpart in the reference, which returns the
+   triangulation of the whole box, kernel.cu:5443-5448).  For a mesh with
+   constraint flags (gcdt_triangulate's output), d_depth[t] receives the
+   fewest constraint edges that a path of triangles crosses from the box
+   edge to triangle t: odd = inside the constrained polygons by the even-odd
+   rule, even > 0 = a hole, 0 = outside every polygon; -1 where no path from
+   the box edge reaches t.  *max_depth (host, may be NULL) receives the
+   greatest depth.  d_scratch (256-byte aligned) holds at least
+   gcdt_classify_regions_scratch_bytes(n_tris) bytes and must not overlap
+   d_depth.  Runs on the current device; returns when d_depth is complete on
+   `stream` (one 4-byte read back per depth level).  GCDT_BAD_INPUT for a
+   neighbour id outside -1..n_tris-1, GCDT_OOM for too little scratch. */
+size_t gcdt_classify_regions_scratch_bytes(int32_t n_tris);
+gcdt_status gcdt_classify_regions(const int32_t* d_adj, const uint8_t* d_cflags, int32_t n_tris,
+                                  int32_t* d_depth, int32_t* max_depth, void* d_scratch,
+                                  size_t scratch_bytes, void* stream);
+
 /* ---- Batched triangulation (no counterpart in the reference, which
    triangulates one point set per process, kernel.cu:5332-5466).
    Many independent instances in one launch: one segmented Morton sort,
