@@ -515,6 +515,75 @@ def run_batched(args):
     bt.close()
 
 
+def run_export(args):
+    """The output-side calls on the scale workload's mesh (10.2M points,
+    20.4M triangles), inputs resident: gcdt_reference_layout (the reference's
+    Morton-renumbered layout with adjacency and flags) and
+    gcdt_classify_regions (even-odd depth).  Algorithmic bytes per call:
+    layout reads points, tris, adj, flags and writes points, labels, tris,
+    adj, flags (8N + 25T + 12(N+4) + 25T); classification reads adj and
+    flags and writes depth (17T)."""
+    import torch
+    import gcdt_b200 as g
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    xy, cons = replica_workload(rank, args.scale_points)
+    n = len(xy)
+    tri = g.Triangulator(max_points=n, max_segments=len(cons), device=local)
+    d_xy = torch.from_numpy(xy).to(dev)
+    tris, adj, cf = tri.triangulate(d_xy, torch.from_numpy(cons).to(dev))
+    tri.close()
+    T = int(tris.shape[0])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    peak, peak_kind = peaks()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        ms = []
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()                         # both calls return once their result is complete
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.median(ms)
+
+    depth_box = {}
+
+    def classify():
+        depth_box["d"], depth_box["max"] = g.classify_regions(adj, cf)
+
+    lay_ms = timed(lambda: g.reference_layout(d_xy, tris, adj, cf))
+    reg_ms = timed(classify)
+    lay_bytes = 8 * n + 25 * T + 12 * (n + 4) + 25 * T
+    reg_bytes = 17 * T
+    inside = int((depth_box["d"] & 1).sum().item())
+    line = {
+        "metric": "output-side calls on the scale mesh", "unit": "ms", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD if not args.scale_points else "reduced: %d generated points" % args.scale_points,
+                   "n_points": n, "n_triangles": T, "l2": "256 MB buffer written between timed steps"},
+        "reference_layout": {"ms": lay_ms, "algorithmic_bytes": lay_bytes,
+                             "roofline": {"bound": "hbm", "achieved": lay_bytes / (lay_ms * 1e-3) / 1e9,
+                                          "peak": peak, "unit": "GB/s",
+                                          "frac": lay_bytes / (lay_ms * 1e-3) / 1e9 / peak,
+                                          "peak_source": peak_kind}},
+        "classify_regions": {"ms": reg_ms, "algorithmic_bytes": reg_bytes, "max_depth": depth_box["max"],
+                             "inside_triangles": inside,
+                             "roofline": {"bound": "hbm", "achieved": reg_bytes / (reg_ms * 1e-3) / 1e9,
+                                          "peak": peak, "unit": "GB/s",
+                                          "frac": reg_bytes / (reg_ms * 1e-3) / 1e9 / peak,
+                                          "peak_source": peak_kind}},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_serving(args):
     """Serving stream: requests with point counts log-uniform in
     [1,000, 1,000,000] (the scale workload's Gaussian/uniform mix in
@@ -595,9 +664,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="scale", choices=["scale", "batched", "serving"],
+    ap.add_argument("--workload", default="scale", choices=["scale", "batched", "serving", "export"],
                     help="scale: the headline 10M-point solve; batched: 4,096 independent instances; "
-                         "serving: a Poisson request stream")
+                         "serving: a Poisson request stream; export: the reference-layout and "
+                         "region-classification calls on the scale mesh")
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--pool", type=int, default=256)
@@ -617,6 +687,8 @@ def main():
         run_batched(args)
     elif args.workload == "serving":
         run_serving(args)
+    elif args.workload == "export":
+        run_export(args)
     else:
         run_ours(args)
 
