@@ -134,6 +134,10 @@ def lib():
     L.gcdt_reference_layout_scratch_bytes.restype = ctypes.c_size_t
     L.gcdt_reference_layout.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
     L.gcdt_reference_layout.restype = ctypes.c_int
+    L.gcdt_set_limits.argtypes = [vp, i32, i32, i32]
+    L.gcdt_set_limits.restype = ctypes.c_int
+    L.gcdt_probe_barrier.argtypes = [ctypes.c_int, i32, i32, ctypes.c_uint32, ctypes.POINTER(i32)]
+    L.gcdt_probe_barrier.restype = ctypes.c_int
     L.gcdt_classify_regions_scratch_bytes.argtypes = [i32]
     L.gcdt_classify_regions_scratch_bytes.restype = ctypes.c_size_t
     L.gcdt_classify_regions.argtypes = [vp, vp, i32, vp, ctypes.POINTER(i32), vp, ctypes.c_size_t, vp]
@@ -305,6 +309,13 @@ class Triangulator:
         tris, adj, cflags = self.triangulate(p, sgm)
         return tris.cpu().numpy(), adj.cpu().numpy(), cflags.cpu().numpy()
 
+    def set_limits(self, insertion_rounds=0, flip_subrounds=0, constraint_rounds=0):
+        """Budgets of the solve's bounded loops (0: the built-in bound); a
+        solve that runs one out raises GcdtError ITER_LIMIT."""
+        rc = lib().gcdt_set_limits(self._h, int(insertion_rounds), int(flip_subrounds), int(constraint_rounds))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_set_limits")
+
     def phase_profile(self):
         """{phase name: (SM cycles, runs)} of the last solve's persistent kernel."""
         cyc = np.zeros(32, np.int64)
@@ -372,6 +383,16 @@ def reference_layout(points, tris, adj=None, cflags=None, stream=None):
     if rc != 0:
         raise GcdtError(rc, "gcdt_reference_layout")
     return pts_out, labels, tris_out, adj_out, cf_out
+
+
+def probe_barrier(device=0, blocks=4, absent_block=0, spin_limit=1 << 16):
+    """Run one grid barrier of the persistent kernel's executor with
+    `absent_block` missing (-1: none); True if the waits ran out."""
+    out = ctypes.c_int32(0)
+    rc = lib().gcdt_probe_barrier(int(device), int(blocks), int(absent_block), int(spin_limit), ctypes.byref(out))
+    if rc != 0:
+        raise GcdtError(rc, "gcdt_probe_barrier")
+    return bool(out.value)
 
 
 def classify_regions(adj, cflags, stream=None):

@@ -31,15 +31,17 @@ struct GridExec {
     // the same L2 line.
     static constexpr int kSnapWords = 12;   // 96 bytes: status..cur_scr
     unsigned long long* snap;                // shared memory, kSnapWords entries
+    unsigned spin_limit = 1u << 24;          // polls before a barrier wait gives up
 
     __device__ void take_snapshot() {
         volatile unsigned long long* src = reinterpret_cast<volatile unsigned long long*>(cnt);
         for (int k = 0; k < kSnapWords; ++k) snap[k] = src[k];
     }
 
-    // Sense-free generation barrier.  Every wait is bounded: after ~2^24
-    // polls the block records ST_BARRIER and stops waiting, and once that bit
-    // is set no block waits or works any more, so the kernel always ends.
+    // Sense-free generation barrier.  Every wait is bounded: after
+    // spin_limit polls (2^24, about a second, in a solve) the block records
+    // ST_BARRIER and stops waiting, and once that bit is set no block waits
+    // or works any more, so the kernel always ends.
     __device__ void barrier() {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -56,7 +58,7 @@ struct GridExec {
                 } else {
                     unsigned spins = 0;
                     while (*vgen == g) {
-                        if (++spins > (1u << 24)) { atomicOr(&cnt->status, ST_BARRIER); break; }
+                        if (++spins > spin_limit) { atomicOr(&cnt->status, ST_BARRIER); break; }
                         if (*vst & ST_BARRIER) break;
                         __nanosleep(64);
                     }

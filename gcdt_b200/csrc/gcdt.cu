@@ -47,6 +47,17 @@ __global__ void __launch_bounds__(kPersistBlock, 1) gcdt_stages(Ctx c) {
     run_stages(ex, c);
 }
 
+// Failure-detection probe of the grid barrier: every block but `absent`
+// enters one barrier of the solver's executor, polling at most spin_limit
+// times.  With a block absent the others' waits run out and record
+// ST_BARRIER; the kernel still ends and the context stays usable.
+__global__ void gcdt_barrier_probe(Counters* cnt, unsigned absent, unsigned spin_limit) {
+    __shared__ unsigned long long snap[GridExec::kSnapWords];
+    GridExec ex{cnt, gridDim.x, snap, spin_limit};
+    if (blockIdx.x == absent) return;
+    ex.barrier();
+}
+
 constexpr int ST_CUDA = 32;
 
 struct DeviceBackend {
@@ -144,6 +155,8 @@ struct gcdt_context {
     int32_t pend_n = 0, pend_s = 0;
     long long pend_launches = 0;
     cudaError_t pend_err = cudaSuccess;
+    // budgets of the bounded loops (gcdt_set_limits; 0 = built-in bound)
+    int32_t lim_rounds = 0, lim_subrounds = 0, lim_crounds = 0;
 };
 
 namespace {
@@ -221,6 +234,9 @@ extern "C" gcdt_status gcdt_triangulate_async(gcdt_context* ctx, const int32_t* 
     c.out_tris = d_tris;
     c.out_adj = d_adj;
     c.out_cflags = d_cflags;
+    c.lim_rounds = ctx->lim_rounds;
+    c.lim_subrounds = ctx->lim_subrounds;
+    c.lim_crounds = ctx->lim_crounds;
     DeviceBackend bk;
     bk.st = static_cast<cudaStream_t>(stream);
     bk.dcnt = c.cnt;
@@ -309,6 +325,38 @@ extern "C" gcdt_status gcdt_eval_predicates(const int32_t* d_quads, int32_t n_ca
     gcdt_predicates<<<(n_cases + 255) / 256, 256, 0, st>>>(reinterpret_cast<const int2*>(d_quads), n_cases, d_out);
     if (cudaGetLastError() != cudaSuccess) return GCDT_CUDA_ERROR;
     if (cudaStreamSynchronize(st) != cudaSuccess) return GCDT_CUDA_ERROR;
+    return GCDT_OK;
+}
+
+extern "C" gcdt_status gcdt_set_limits(gcdt_context* ctx, int32_t max_insertion_rounds,
+                                       int32_t max_flip_subrounds, int32_t max_constraint_rounds) {
+    if (!ctx || max_insertion_rounds < 0 || max_flip_subrounds < 0 || max_constraint_rounds < 0)
+        return GCDT_BAD_INPUT;
+    ctx->lim_rounds = max_insertion_rounds;
+    ctx->lim_subrounds = max_flip_subrounds;
+    ctx->lim_crounds = max_constraint_rounds;
+    return GCDT_OK;
+}
+
+extern "C" gcdt_status gcdt_probe_barrier(int device, int32_t blocks, int32_t absent_block, uint32_t spin_limit,
+                                          int32_t* timed_out) {
+    if (!timed_out || blocks < 1 || blocks > 1024 || spin_limit == 0) return GCDT_BAD_INPUT;
+    *timed_out = 0;
+    DeviceGuard g(device);
+    Counters* cnt = nullptr;
+    if (cudaMalloc(&cnt, sizeof(Counters)) != cudaSuccess) return GCDT_CUDA_ERROR;
+    cudaError_t e = cudaMemset(cnt, 0, sizeof(Counters));
+    if (e == cudaSuccess) {
+        unsigned absent = absent_block < 0 ? 0xffffffffu : (unsigned)absent_block;
+        gcdt_barrier_probe<<<blocks, 32>>>(cnt, absent, spin_limit);
+        e = cudaGetLastError();
+    }
+    int status = 0;
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&status, &cnt->status, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(cnt);
+    if (e != cudaSuccess) return GCDT_CUDA_ERROR;
+    *timed_out = (status & ST_BARRIER) ? 1 : 0;
     return GCDT_OK;
 }
 

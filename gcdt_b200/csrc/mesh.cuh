@@ -137,6 +137,13 @@ struct Ctx {
     int* out_adj;
     unsigned char* out_cflags;
 
+    // Budgets of the bounded driver loops (0: the built-in bound): grid
+    // insertion rounds per solve, flip sub-rounds per flip loop, constraint
+    // rounds.  A budget that runs out ends the solve with ST_ITER_LIMIT.
+    int lim_rounds;
+    int lim_subrounds;
+    int lim_crounds;
+
     Counters* cnt;
 };
 

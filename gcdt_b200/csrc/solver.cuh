@@ -121,6 +121,19 @@ constexpr long long kCarryQueue = 1 << 22;
 constexpr long long kMaxRounds = 1 << 16;
 constexpr unsigned kMaxConstraintRounds = 1 << 14;
 
+// The budgets a solve runs under: the context's, where set and within the
+// built-in bound (the constraint rounds' bound also spaces the queue stamps).
+GCDT_HD long long budget_subrounds(const Ctx& c) {
+    return c.lim_subrounds > 0 && c.lim_subrounds < kMaxSubrounds ? c.lim_subrounds : kMaxSubrounds;
+}
+GCDT_HD long long budget_rounds(const Ctx& c) {
+    return c.lim_rounds > 0 && c.lim_rounds < kMaxRounds ? c.lim_rounds : kMaxRounds;
+}
+GCDT_HD unsigned budget_crounds(const Ctx& c) {
+    return c.lim_crounds > 0 && (unsigned)c.lim_crounds < kMaxConstraintRounds ? (unsigned)c.lim_crounds
+                                                                              : kMaxConstraintRounds;
+}
+
 // The stage driver runs the same control flow on every GPU thread of the
 // persistent kernel (EX = grid executor: a phase is a grid-stride loop
 // followed by a grid barrier) and on the host for the CPU emulation
@@ -163,8 +176,9 @@ GCDT_HD void run_phase(EX& ex, Ctx& c, Driver& D, int k, long long count) {
 template <class EX>
 GCDT_HD int flip_loop(EX& ex, Ctx& c, Driver& D, long long& nq, long long max_nq, long long stop = 0) {
     long long guard = 0;
+    const long long budget = budget_subrounds(c);
     while (nq > 0 && nq <= max_nq && (guard == 0 || nq > stop)) {
-        if (++guard > kMaxSubrounds) return ST_ITER_LIMIT;
+        if (++guard > budget) return ST_ITER_LIMIT;
         if (EX::kCanNarrow && nq <= kNarrowQueue) {
             int rc = ex.narrow_flips(c, D, nq);
             if (rc || D.errs) return rc ? rc : D.errs;
@@ -212,7 +226,7 @@ GCDT_HD int insert_rounds(EX& ex, Ctx& c, Driver& D, long long nact) {
             }
             return ex.narrow_rounds(c, D, nact);
         }
-        if (++D.round > kMaxRounds) return ST_ITER_LIMIT;
+        if (++D.round > budget_rounds(c)) return ST_ITER_LIMIT;
         c.round = D.round;
         c.act = D.actA; c.act_next = D.actB;
         c.base_act = D.e_act;
@@ -268,8 +282,9 @@ GCDT_HD int insert_constraints(EX& ex, Ctx& c, Driver& D) {
     c.lq = D.qa;
     c.base_law = D.e_law;
     unsigned cr = 0;
+    const unsigned cbudget = budget_crounds(c);
     while (npend > 0) {
-        if (++cr > kMaxConstraintRounds) return ST_ITER_LIMIT;
+        if (++cr > cbudget) return ST_ITER_LIMIT;
         D.sr++;
         c.sr = D.sr;
         c.pend = pa; c.pend_next = pb;

@@ -106,6 +106,26 @@ gcdt_status gcdt_wait(gcdt_context* ctx, int32_t* n_tris);
 gcdt_status gcdt_get_stats(const gcdt_context* ctx, gcdt_stats* out);
 const char* gcdt_status_string(gcdt_status s);
 
+/* Budgets of the solve's bounded loops on ctx (0 = the built-in bound, which
+   is also the ceiling): grid insertion rounds per solve, flip sub-rounds per
+   flip pass, constraint-recovery rounds.  A solve that runs a budget out
+   returns GCDT_ITER_LIMIT and leaves the context usable; the reference's
+   counterparts are its fixed caps (multiFlipFE count > 10, kernel.cu:3667;
+   locateStart 10000 steps, addConstraints.cu:769-773), after which it drops
+   the work silently. */
+gcdt_status gcdt_set_limits(gcdt_context* ctx, int32_t max_insertion_rounds,
+                            int32_t max_flip_subrounds, int32_t max_constraint_rounds);
+
+/* Failure-detection probe of the persistent kernel's grid barrier on
+   `device`: `blocks` blocks enter one barrier, except absent_block (-1:
+   none), each polling at most spin_limit times.  *timed_out = 1 when the
+   waits ran out (the barrier records its timeout status and the kernel ends
+   normally), 0 when the barrier completed.  Allocates and frees one small
+   device buffer; synchronizes the device.  No counterpart in the reference,
+   whose waits are unbounded. */
+gcdt_status gcdt_probe_barrier(int device, int32_t blocks, int32_t absent_block, uint32_t spin_limit,
+                               int32_t* timed_out);
+
 /* Per-phase profile of the last solve on ctx: SM cycles spent in each phase
    kind of the persistent stage kernel (measured by block 0, barrier wait
    included) and how often it ran.  Returns the number of phase kinds

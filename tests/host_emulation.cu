@@ -25,6 +25,7 @@ int g_width = 1;          // items per call in the flip passes (1: one-item bodi
 bool g_check = false;     // mesh consistency after every split fix and flip fix
 int g_bad = 0;
 std::mt19937 g_rng(1);
+int g_lim[3] = {0, 0, 0};   // loop budgets of the next solves (0: built-in bound)
 
 // Every live triangle CCW, every adjacency mutual.
 void check_mesh(int kind, const Ctx& c) {
@@ -151,6 +152,9 @@ extern "C" int host_triangulate(const int* xy, int n, const int* cons, int s, in
     c.out_tris = tris;
     c.out_adj = adj;
     c.out_cflags = cflags;
+    c.lim_rounds = g_lim[0];
+    c.lim_subrounds = g_lim[1];
+    c.lim_crounds = g_lim[2];
     HostBackend bk{c.cnt};
     SolveStats ss;
     int rc = run_solve(bk, c, ss);
@@ -160,4 +164,11 @@ extern "C" int host_triangulate(const int* xy, int n, const int* cons, int s, in
     stats[3] = ss.flips;
     stats[4] = ss.constraint_rounds;
     return g_bad ? 1000 + g_bad : rc;
+}
+
+// Loop budgets for the following host solves, as gcdt_set_limits.
+extern "C" void host_set_limits(int rounds, int subrounds, int crounds) {
+    g_lim[0] = rounds;
+    g_lim[1] = subrounds;
+    g_lim[2] = crounds;
 }
