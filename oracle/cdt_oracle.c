@@ -132,6 +132,22 @@ int oracle_incircle_sos(const int64_t *xy4)
     return incircle_sos_v(&m, 0, 1, 2, 3);
 }
 
+/* The three predicates of n cases: quads holds 8 int32 per case (points a,
+   b, c, d); out receives orient2d(a,b,c), incircle(a,b,c,d) and the
+   perturbed incircle(a,b,c,d), 3 int32 per case -- the layout of the
+   device's gcdt_eval_predicates. */
+void oracle_predicates_batch(const int32_t *quads, int64_t n, int32_t *out)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        const int32_t *q = quads + 8 * i;
+        int64_t xy4[8];
+        for (int k = 0; k < 8; ++k) xy4[k] = q[k];
+        out[3 * i] = oracle_orient(xy4[0], xy4[1], xy4[2], xy4[3], xy4[4], xy4[5]);
+        out[3 * i + 1] = oracle_incircle(xy4[0], xy4[1], xy4[2], xy4[3], xy4[4], xy4[5], xy4[6], xy4[7]);
+        out[3 * i + 2] = oracle_incircle_sos(xy4);
+    }
+}
+
 /* ---------------------------------------------------------------- mesh ops */
 
 static int push(mesh_t *m, int t, int s)

@@ -39,6 +39,8 @@ def _lib():
         O.oracle_incircle.restype = ctypes.c_int
         O.oracle_incircle_sos.argtypes = [vp]
         O.oracle_incircle_sos.restype = ctypes.c_int
+        O.oracle_predicates_batch.argtypes = [vp, ctypes.c_int64, vp]
+        O.oracle_predicates_batch.restype = None
         _O = O
     return _O
 
@@ -86,3 +88,12 @@ def incircle(a, b, c, d):
 def incircle_sos(a, b, c, d):
     q = np.array([a, b, c, d], dtype=np.int64).reshape(8)
     return _lib().oracle_incircle_sos(_p(q))
+
+
+def predicates_batch(quads):
+    """quads: (k, 4, 2) int32 -> (k, 3) int32 of [orient2d(a,b,c),
+    incircle(a,b,c,d), perturbed incircle(a,b,c,d)], exact."""
+    q = np.ascontiguousarray(quads, dtype=np.int32).reshape(-1, 8)
+    out = np.zeros((len(q), 3), np.int32)
+    _lib().oracle_predicates_batch(_p(q), len(q), _p(out))
+    return out

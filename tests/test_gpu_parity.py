@@ -118,3 +118,21 @@ def test_predicates_bit_equal_to_oracle():
         assert dev[i, 0] == oracle.orient(a, b, c), i
         assert dev[i, 1] == oracle.incircle(a, b, c, d4), i
         assert dev[i, 2] == oracle.incircle_sos(a, b, c, d4), i
+
+
+def test_predicates_bit_equal_on_1e8_cases():
+    """10^8 seeded cases (uniform, tiny clusters, cocircular, collinear and
+    one-unit perturbations of cocircular quads), in chunks of 10^7: the
+    device's orient2d, inCircle and perturbed inCircle equal the exact
+    oracle on every case."""
+    from tests.predicate_cases import predicate_cases
+    rng = np.random.default_rng(2026)
+    zeros = 0
+    for _ in range(10):
+        q = predicate_cases(rng, 10_000_000)
+        dev = g.eval_predicates(q)
+        ref = oracle.predicates_batch(q)
+        bad = np.nonzero((dev != ref).any(axis=1))[0]
+        assert len(bad) == 0, (bad[:5], q[bad[:5]].tolist(), dev[bad[:5]].tolist(), ref[bad[:5]].tolist())
+        zeros += int((ref[:, 1] == 0).sum())
+    assert zeros > 10_000_000

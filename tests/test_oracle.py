@@ -182,3 +182,17 @@ def test_golden_fixtures():
         rc, tris, adj, cf, _ = oracle.cdt(xy, cons)
         assert rc == 0
         assert g.canonical(tris).tolist() == case["canonical_tris"], case["name"]
+
+
+def test_batched_predicates_equal_python_ints():
+    """oracle.predicates_batch (the checker of the device predicates on
+    10^8 cases) against independent Python-integer arithmetic."""
+    from tests.predicate_cases import predicate_cases
+    q = predicate_cases(np.random.default_rng(5), 6000)
+    out = oracle.predicates_batch(q)
+    for i in range(len(q)):
+        a, b, c, d = (tuple(int(v) for v in p) for p in q[i])
+        assert out[i, 0] == bf.orient(a, b, c)
+        assert out[i, 1] == bf.incircle(a, b, c, d)
+        assert out[i, 2] == bf.incircle_sos(a, b, c, d)
+    assert (out[:, 1] == 0).sum() > 1000          # the degenerate shapes are present
