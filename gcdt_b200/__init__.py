@@ -39,6 +39,18 @@ class GcdtError(RuntimeError):
         super().__init__("%s: %s" % (what or "gcdt", self.status))
 
 
+class Tuning(ctypes.Structure):
+    """gcdt_tuning: scheduling of a context's solves (include/gcdt.h)."""
+    _fields_ = [("levels", ctypes.c_int32), ("level_stride", ctypes.c_int32 * 3),
+                ("carry_queue", ctypes.c_int32), ("narrow_queue", ctypes.c_int32),
+                ("narrow_active", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {"levels": self.levels, "level_stride": list(self.level_stride)[:max(self.levels - 1, 0)],
+                "carry_queue": self.carry_queue, "narrow_queue": self.narrow_queue,
+                "narrow_active": self.narrow_active}
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("n_points", ctypes.c_int64), ("n_segments", ctypes.c_int64),
@@ -134,6 +146,10 @@ def lib():
     L.gcdt_reference_layout_scratch_bytes.restype = ctypes.c_size_t
     L.gcdt_reference_layout.argtypes = [vp, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]
     L.gcdt_reference_layout.restype = ctypes.c_int
+    L.gcdt_set_tuning.argtypes = [vp, vp]
+    L.gcdt_set_tuning.restype = ctypes.c_int
+    L.gcdt_get_tuning.argtypes = [vp, vp]
+    L.gcdt_get_tuning.restype = ctypes.c_int
     L.gcdt_set_limits.argtypes = [vp, i32, i32, i32]
     L.gcdt_set_limits.restype = ctypes.c_int
     L.gcdt_probe_barrier.argtypes = [ctypes.c_int, i32, i32, ctypes.c_uint32, ctypes.POINTER(i32)]
@@ -315,6 +331,37 @@ class Triangulator:
         rc = lib().gcdt_set_limits(self._h, int(insertion_rounds), int(flip_subrounds), int(constraint_rounds))
         if rc != 0:
             raise GcdtError(rc, "gcdt_set_limits")
+
+    def set_tuning(self, levels=None, level_stride=None, carry_queue=None, narrow_queue=None,
+                   narrow_active=None):
+        """Change the scheduling of later solves (unnamed fields keep their
+        value); set_tuning() with no argument restores the defaults."""
+        if all(v is None for v in (levels, level_stride, carry_queue, narrow_queue, narrow_active)):
+            rc = lib().gcdt_set_tuning(self._h, None)
+        else:
+            t = Tuning()
+            lib().gcdt_get_tuning(self._h, ctypes.byref(t))
+            if levels is not None:
+                t.levels = int(levels)
+            if level_stride is not None:
+                for k, v in enumerate(list(level_stride)[:3]):
+                    t.level_stride[k] = int(v)
+            if carry_queue is not None:
+                t.carry_queue = int(carry_queue)
+            if narrow_queue is not None:
+                t.narrow_queue = int(narrow_queue)
+            if narrow_active is not None:
+                t.narrow_active = int(narrow_active)
+            rc = lib().gcdt_set_tuning(self._h, ctypes.byref(t))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_set_tuning")
+
+    def tuning(self):
+        t = Tuning()
+        rc = lib().gcdt_get_tuning(self._h, ctypes.byref(t))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_get_tuning")
+        return t.as_dict()
 
     def phase_profile(self):
         """{phase name: (SM cycles, runs)} of the last solve's persistent kernel."""

@@ -165,7 +165,7 @@ __device__ inline int GridExec::narrow_flips(Ctx& c, Driver& D, long long& nq) {
         Driver Db = D;
         Ctx cb = c;
         long long left = nq;
-        int rc = flip_loop(bx, cb, Db, left, 4 * kNarrowQueue);
+        int rc = flip_loop(bx, cb, Db, left, 4 * (long long)c.narrow_q);
         if (threadIdx.x == 0) store_handoff(cnt, Db, left, rc);
     }
     barrier();

@@ -142,6 +142,20 @@ inline gcdt_status map_status(int bits) {
 
 using namespace gcdt;
 
+namespace {
+gcdt_tuning default_tuning() {
+    gcdt_tuning t{};
+    t.levels = 3;
+    t.level_stride[0] = 512;
+    t.level_stride[1] = 8;
+    t.level_stride[2] = 1;
+    t.carry_queue = (int32_t)kCarryQueue;
+    t.narrow_queue = (int32_t)kNarrowQueue;
+    t.narrow_active = (int32_t)kNarrowActive;
+    return t;
+}
+}  // namespace
+
 struct gcdt_context {
     int device = 0;
     int64_t max_n = 0, max_s = 0;
@@ -157,6 +171,8 @@ struct gcdt_context {
     cudaError_t pend_err = cudaSuccess;
     // budgets of the bounded loops (gcdt_set_limits; 0 = built-in bound)
     int32_t lim_rounds = 0, lim_subrounds = 0, lim_crounds = 0;
+    // scheduling (gcdt_set_tuning)
+    gcdt_tuning tuning = default_tuning();
 };
 
 namespace {
@@ -237,6 +253,14 @@ extern "C" gcdt_status gcdt_triangulate_async(gcdt_context* ctx, const int32_t* 
     c.lim_rounds = ctx->lim_rounds;
     c.lim_subrounds = ctx->lim_subrounds;
     c.lim_crounds = ctx->lim_crounds;
+    {
+        const gcdt_tuning& t = ctx->tuning;
+        c.nlevels = t.levels;
+        for (int k = 0; k < 4; ++k) c.stride[k] = k < 3 && k + 1 < t.levels ? t.level_stride[k] : 1;
+        c.carry_q = t.carry_queue;
+        c.narrow_q = t.narrow_queue;
+        c.narrow_act = t.narrow_active;
+    }
     DeviceBackend bk;
     bk.st = static_cast<cudaStream_t>(stream);
     bk.dcnt = c.cnt;
@@ -335,6 +359,29 @@ extern "C" gcdt_status gcdt_set_limits(gcdt_context* ctx, int32_t max_insertion_
     ctx->lim_rounds = max_insertion_rounds;
     ctx->lim_subrounds = max_flip_subrounds;
     ctx->lim_crounds = max_constraint_rounds;
+    return GCDT_OK;
+}
+
+extern "C" gcdt_status gcdt_set_tuning(gcdt_context* ctx, const gcdt_tuning* tuning) {
+    if (!ctx) return GCDT_BAD_INPUT;
+    if (!tuning) { ctx->tuning = default_tuning(); return GCDT_OK; }
+    const gcdt_tuning& t = *tuning;
+    if (t.levels < 1 || t.levels > 4) return GCDT_BAD_INPUT;
+    for (int k = 0; k + 1 < t.levels; ++k) {
+        if (t.level_stride[k] < 2) return GCDT_BAD_INPUT;
+        if (k > 0 && t.level_stride[k] >= t.level_stride[k - 1]) return GCDT_BAD_INPUT;
+    }
+    if (t.carry_queue < 0 || t.carry_queue > (1 << 24)) return GCDT_BAD_INPUT;
+    if (t.narrow_queue < 0 || t.narrow_queue > 65536 || t.narrow_active < 0 || t.narrow_active > 65536)
+        return GCDT_BAD_INPUT;
+    ctx->tuning = t;
+    for (int k = t.levels - 1; k < 3; ++k) ctx->tuning.level_stride[k] = 1;
+    return GCDT_OK;
+}
+
+extern "C" gcdt_status gcdt_get_tuning(const gcdt_context* ctx, gcdt_tuning* tuning) {
+    if (!ctx || !tuning) return GCDT_BAD_INPUT;
+    *tuning = ctx->tuning;
     return GCDT_OK;
 }
 

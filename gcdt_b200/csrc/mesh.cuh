@@ -144,6 +144,15 @@ struct Ctx {
     int lim_subrounds;
     int lim_crounds;
 
+    // Scheduling of the whole-grid solve (set by bind_ctx, tunable per
+    // context): flip sub-rounds of a round stop once the queue is at most
+    // carry_q long (the rest is carried into the next round; 0: never);
+    // flip queues of at most narrow_q entries and insertion tails of at most
+    // narrow_act points run in one block (0: never).
+    int carry_q;
+    int narrow_q;
+    int narrow_act;
+
     Counters* cnt;
 };
 

@@ -37,6 +37,23 @@ struct SolveStats {
     long long host_syncs = 0;
 };
 
+constexpr long long kMaxSubrounds = 1 << 20;
+// A flip queue or an active list this short is finished by one block with
+// block barriers instead of the whole grid with grid barriers.
+constexpr long long kNarrowQueue = 1024;
+constexpr long long kNarrowActive = 1024;
+// On the whole grid, a round's flip sub-rounds stop (after the first) once
+// the queue has at most this many entries; the rest of the queue is carried
+// into the next round's first flip queue and drained before the level ends
+// or the insertion tail moves to one block, so the shrinking sub-rounds of
+// one round run together with the next round's large first one.  Insertion
+// and location work on any triangulation; only the final mesh must be
+// Delaunay.  (Measured on the 10M-point workload: 1K 33.0 ms, 64K 31.6,
+// 256K 31.3, 4M 30.8, 16M 31.3; no carry 35.4.)
+constexpr long long kCarryQueue = 1 << 22;
+constexpr long long kMaxRounds = 1 << 16;
+constexpr unsigned kMaxConstraintRounds = 1 << 14;
+
 __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     Ctx c{};
     c.n = (int)p.n; c.s = (int)p.s; c.ntri = (int)p.ntri;
@@ -74,6 +91,9 @@ __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     // endpoints, then every 8th, then the rest
     c.nlevels = 3;
     c.stride[0] = 512; c.stride[1] = 8; c.stride[2] = 1; c.stride[3] = 1;
+    c.carry_q = (int)kCarryQueue;
+    c.narrow_q = (int)kNarrowQueue;
+    c.narrow_act = (int)kNarrowActive;
     return c;
 }
 
@@ -104,22 +124,6 @@ GCDT_HD void dispatch(int k, const Ctx& c, int i) {
     }
 }
 
-constexpr long long kMaxSubrounds = 1 << 20;
-// A flip queue or an active list this short is finished by one block with
-// block barriers instead of the whole grid with grid barriers.
-constexpr long long kNarrowQueue = 1024;
-constexpr long long kNarrowActive = 1024;
-// On the whole grid, a round's flip sub-rounds stop (after the first) once
-// the queue has at most this many entries; the rest of the queue is carried
-// into the next round's first flip queue and drained before the level ends
-// or the insertion tail moves to one block, so the shrinking sub-rounds of
-// one round run together with the next round's large first one.  Insertion
-// and location work on any triangulation; only the final mesh must be
-// Delaunay.  (Measured on the 10M-point workload: 1K 33.0 ms, 64K 31.6,
-// 256K 31.3, 4M 30.8, 16M 31.3; no carry 35.4.)
-constexpr long long kCarryQueue = 1 << 22;
-constexpr long long kMaxRounds = 1 << 16;
-constexpr unsigned kMaxConstraintRounds = 1 << 14;
 
 // The budgets a solve runs under: the context's, where set and within the
 // built-in bound (the constraint rounds' bound also spaces the queue stamps).
@@ -179,7 +183,7 @@ GCDT_HD int flip_loop(EX& ex, Ctx& c, Driver& D, long long& nq, long long max_nq
     const long long budget = budget_subrounds(c);
     while (nq > 0 && nq <= max_nq && (guard == 0 || nq > stop)) {
         if (++guard > budget) return ST_ITER_LIMIT;
-        if (EX::kCanNarrow && nq <= kNarrowQueue) {
+        if (EX::kCanNarrow && nq <= c.narrow_q) {
             int rc = ex.narrow_flips(c, D, nq);
             if (rc || D.errs) return rc ? rc : D.errs;
             continue;
@@ -215,7 +219,7 @@ GCDT_HD int flip_until_delaunay(EX& ex, Ctx& c, Driver& D, long long nq) {
 template <class EX>
 GCDT_HD int insert_rounds(EX& ex, Ctx& c, Driver& D, long long nact) {
     while (nact > 0) {
-        if (EX::kCanNarrow && nact <= kNarrowActive) {
+        if (EX::kCanNarrow && nact <= c.narrow_act) {
             // the single-block tail starts from a Delaunay mesh: the carried
             // flips are finished by the whole grid first
             if (D.carry > 0) {
@@ -253,7 +257,7 @@ GCDT_HD int insert_rounds(EX& ex, Ctx& c, Driver& D, long long nact) {
         long long nq = (long long)(D.e_q - c.base_q);
         D.drop = D.carry;
         D.carry = 0;
-        int rc = flip_loop(ex, c, D, nq, (long long)1 << 62, EX::kCanNarrow ? kCarryQueue : 0);
+        int rc = flip_loop(ex, c, D, nq, (long long)1 << 62, EX::kCanNarrow ? (long long)c.carry_q : 0);
         if (rc) return rc;
         D.carry = nq;
     }

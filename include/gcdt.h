@@ -116,6 +116,33 @@ const char* gcdt_status_string(gcdt_status s);
 gcdt_status gcdt_set_limits(gcdt_context* ctx, int32_t max_insertion_rounds,
                             int32_t max_flip_subrounds, int32_t max_constraint_rounds);
 
+/* Scheduling of a context's solves (the output does not depend on it: the
+   constrained Delaunay triangulation is unique under the fixed tie-break).
+     levels          insertion levels, 1..4;
+     level_stride    level k < levels-1 holds every level_stride[k]-th point
+                     of the Morton order not in a lower level (plus, for
+                     level 0, every segment endpoint); strictly decreasing,
+                     >= 2; entries from levels-1 on are ignored;
+     carry_queue     a round stops its flip sub-rounds once the queue is at
+                     most this long and carries the rest into the next round
+                     (0: never carry), 0..2^24;
+     narrow_queue    flip queues of at most this many entries run in one
+                     block with block barriers (0: never), 0..65536;
+     narrow_active   insertion tails of at most this many points run in one
+                     block (0: never), 0..65536.
+   Defaults: 3 levels, strides 512 and 8, carry 2^22, narrow 1024 and 1024.
+   The reference fixes its counterparts at compile time (logSample, the
+   bitmap size, QUEUE_SIZE: math_base.cuh:24-26, kernel.cu:2827). */
+typedef struct {
+    int32_t levels;
+    int32_t level_stride[3];
+    int32_t carry_queue;
+    int32_t narrow_queue;
+    int32_t narrow_active;
+} gcdt_tuning;
+gcdt_status gcdt_set_tuning(gcdt_context* ctx, const gcdt_tuning* tuning);   /* NULL: the defaults */
+gcdt_status gcdt_get_tuning(const gcdt_context* ctx, gcdt_tuning* tuning);
+
 /* Failure-detection probe of the persistent kernel's grid barrier on
    `device`: `blocks` blocks enter one barrier, except absent_block (-1:
    none), each polling at most spin_limit times.  *timed_out = 1 when the

@@ -26,6 +26,7 @@ bool g_check = false;     // mesh consistency after every split fix and flip fix
 int g_bad = 0;
 std::mt19937 g_rng(1);
 int g_lim[3] = {0, 0, 0};   // loop budgets of the next solves (0: built-in bound)
+int g_tune[7] = {0};         // scheduling of the next solves: levels, strides[3], carry, narrow q/act (levels 0: default)
 
 // Every live triangle CCW, every adjacency mutual.
 void check_mesh(int kind, const Ctx& c) {
@@ -86,7 +87,7 @@ struct HostGrid {
         Driver Db = D;
         Ctx cb = c;
         long long left = nq;
-        int rc = flip_loop(bx, cb, Db, left, 4 * kNarrowQueue);
+        int rc = flip_loop(bx, cb, Db, left, 4 * (long long)c.narrow_q);
         D = Db;
         nq = left;
         return rc;
@@ -155,6 +156,13 @@ extern "C" int host_triangulate(const int* xy, int n, const int* cons, int s, in
     c.lim_rounds = g_lim[0];
     c.lim_subrounds = g_lim[1];
     c.lim_crounds = g_lim[2];
+    if (g_tune[0] > 0) {
+        c.nlevels = g_tune[0];
+        for (int k = 0; k < 4; ++k) c.stride[k] = k < 3 && k + 1 < c.nlevels ? g_tune[1 + k] : 1;
+        c.carry_q = g_tune[4];
+        c.narrow_q = g_tune[5];
+        c.narrow_act = g_tune[6];
+    }
     HostBackend bk{c.cnt};
     SolveStats ss;
     int rc = run_solve(bk, c, ss);
@@ -171,4 +179,11 @@ extern "C" void host_set_limits(int rounds, int subrounds, int crounds) {
     g_lim[0] = rounds;
     g_lim[1] = subrounds;
     g_lim[2] = crounds;
+}
+
+// Scheduling of the following host solves, as gcdt_set_tuning (levels 0:
+// the defaults).
+extern "C" void host_set_tuning(int levels, int s0, int s1, int s2, int carry, int narrow_q, int narrow_act) {
+    int v[7] = {levels, s0, s1, s2, carry, narrow_q, narrow_act};
+    for (int k = 0; k < 7; ++k) g_tune[k] = v[k];
 }
