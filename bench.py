@@ -265,6 +265,7 @@ def run_ours(args):
     xy, cons = replica_workload(rank, args.scale_points)
     n, s = len(xy), len(cons)
     tri = g.Triangulator(max_points=n, max_segments=s, device=local)
+    apply_tuning(tri, args)
     stream = torch.cuda.current_stream(dev)
 
     d_xy = torch.from_numpy(xy).to(dev)
@@ -335,6 +336,7 @@ def run_ours(args):
     # host memory and its whole mesh back out; the L2 flush stays in front
     # of every solve.
     tri2 = g.Triangulator(max_points=n, max_segments=s, device=local)
+    apply_tuning(tri2, args)
     ctxs = (tri, tri2)
     streams = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
     d_in = ((d_xy, d_cons), (torch.empty_like(d_xy), torch.empty_like(d_cons)))
@@ -397,6 +399,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD if not args.scale_points else "PROFILING ONLY, reduced: %d generated points" % args.scale_points,
                        "n_points": n, "n_segments": s, "n_triangles": T,
                        "parallelism": "replicas (one independent triangulation per GPU)" if world > 1 else "single GPU",
+                       "schedule": tri.tuning(),
                        "l2": "256 MB buffer written between timed steps; working set ~2 GB"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
@@ -423,6 +426,23 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     tri.close()
     dist_done(world)
+
+
+def apply_tuning(tri, args):
+    """The solve's scheduling from the command line (unset: the defaults)."""
+    kw = {}
+    if args.levels is not None:
+        kw["levels"] = args.levels
+    if args.strides is not None:
+        kw["level_stride"] = [int(v) for v in args.strides.split(",")]
+    if args.carry is not None:
+        kw["carry_queue"] = args.carry
+    if args.narrow_queue is not None:
+        kw["narrow_queue"] = args.narrow_queue
+    if args.narrow_active is not None:
+        kw["narrow_active"] = args.narrow_active
+    if kw:
+        tri.set_tuning(**kw)
 
 
 def run_batched(args):
@@ -678,6 +698,11 @@ def main():
     ap.add_argument("--validate", action="store_true")
     ap.add_argument("--scale-points", type=int, default=0,
                     help="profiling only: a reduced copy of the workload with this many generated points")
+    ap.add_argument("--levels", type=int, default=None, help="insertion levels (1-4)")
+    ap.add_argument("--strides", default=None, help="level strides, comma separated, e.g. 512,8")
+    ap.add_argument("--carry", type=int, default=None, help="flip-queue carry threshold (0: never)")
+    ap.add_argument("--narrow-queue", type=int, default=None, help="single-block flip-queue threshold")
+    ap.add_argument("--narrow-active", type=int, default=None, help="single-block insertion-tail threshold")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per solve from an ncu capture, reported as roofline.traffic")
     args = ap.parse_args()
