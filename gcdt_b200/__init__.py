@@ -150,6 +150,8 @@ def lib():
     L.gcdt_set_tuning.restype = ctypes.c_int
     L.gcdt_get_tuning.argtypes = [vp, vp]
     L.gcdt_get_tuning.restype = ctypes.c_int
+    L.gcdt_autotune.argtypes = [vp, vp, i32, vp, i32, vp, vp, vp, i32, vp, vp]
+    L.gcdt_autotune.restype = ctypes.c_int
     L.gcdt_set_limits.argtypes = [vp, i32, i32, i32]
     L.gcdt_set_limits.restype = ctypes.c_int
     L.gcdt_probe_barrier.argtypes = [ctypes.c_int, i32, i32, ctypes.c_uint32, ctypes.POINTER(i32)]
@@ -355,6 +357,20 @@ class Triangulator:
             rc = lib().gcdt_set_tuning(self._h, ctypes.byref(t))
         if rc != 0:
             raise GcdtError(rc, "gcdt_set_tuning")
+
+    def autotune(self, points, segments=None, repeats=2, out=None, stream=None):
+        """Time the candidate schedules on this problem (device tensors) and
+        keep the fastest; returns it as a dict."""
+        points, segments, n, sp, s, out, stream = self._args(points, segments, out, stream)
+        tris, adj, cflags = out
+        t = Tuning()
+        rc = lib().gcdt_autotune(self._h, ctypes.c_void_p(points.data_ptr() if n else 0), int(n),
+                                 ctypes.c_void_p(sp or 0), int(s), ctypes.c_void_p(tris.data_ptr()),
+                                 ctypes.c_void_p(adj.data_ptr()), ctypes.c_void_p(cflags.data_ptr()),
+                                 int(repeats), ctypes.byref(t), ctypes.c_void_p(stream))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_autotune")
+        return t.as_dict()
 
     def tuning(self):
         t = Tuning()

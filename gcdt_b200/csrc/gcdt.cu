@@ -379,6 +379,57 @@ extern "C" gcdt_status gcdt_set_tuning(gcdt_context* ctx, const gcdt_tuning* tun
     return GCDT_OK;
 }
 
+// Candidate schedules of gcdt_autotune: the defaults first, then denser or
+// sparser level strides, two-level schedules and smaller carries.
+namespace {
+gcdt_tuning candidate(int levels, int s0, int s1, int carry) {
+    gcdt_tuning t = default_tuning();
+    t.levels = levels;
+    t.level_stride[0] = s0;
+    t.level_stride[1] = levels > 2 ? s1 : 1;
+    t.level_stride[2] = 1;
+    t.carry_queue = carry;
+    return t;
+}
+}  // namespace
+
+extern "C" gcdt_status gcdt_autotune(gcdt_context* ctx, const int32_t* d_points, int32_t n,
+                                     const int32_t* d_segments, int32_t s, int32_t* d_tris, int32_t* d_adj,
+                                     uint8_t* d_cflags, int32_t repeats, gcdt_tuning* chosen, void* stream) {
+    if (!ctx || repeats < 1 || repeats > 16) return GCDT_BAD_INPUT;
+    const gcdt_tuning cands[] = {
+        default_tuning(),
+        candidate(3, 256, 8, (int)kCarryQueue), candidate(3, 1024, 16, (int)kCarryQueue),
+        candidate(3, 512, 16, (int)kCarryQueue), candidate(3, 256, 4, (int)kCarryQueue),
+        candidate(2, 64, 1, (int)kCarryQueue), candidate(2, 256, 1, (int)kCarryQueue),
+        candidate(3, 512, 8, 1 << 20), candidate(3, 512, 8, 1 << 24),
+    };
+    const gcdt_tuning keep = ctx->tuning;
+    int best = -1;
+    double best_ms = 0.0;
+    int32_t nt = 0;
+    // one untimed solve first (module load, caches), then every candidate
+    ctx->tuning = cands[0];
+    gcdt_status rc = gcdt_triangulate(ctx, d_points, n, d_segments, s, d_tris, d_adj, d_cflags, &nt, stream);
+    for (int k = 0; rc == GCDT_OK && k < (int)(sizeof(cands) / sizeof(cands[0])); ++k) {
+        ctx->tuning = cands[k];
+        double ms = 0.0;
+        for (int r = 0; r < repeats && rc == GCDT_OK; ++r) {
+            rc = gcdt_triangulate(ctx, d_points, n, d_segments, s, d_tris, d_adj, d_cflags, &nt, stream);
+            double m = ctx->stats.device_ms;
+            if (r == 0 || m < ms) ms = m;
+        }
+        if (rc == GCDT_OK && (best < 0 || ms < best_ms)) { best = k; best_ms = ms; }
+    }
+    if (rc != GCDT_OK || best < 0) {
+        ctx->tuning = keep;
+        return rc != GCDT_OK ? rc : GCDT_INTERNAL;
+    }
+    ctx->tuning = cands[best];
+    if (chosen) *chosen = cands[best];
+    return GCDT_OK;
+}
+
 extern "C" gcdt_status gcdt_get_tuning(const gcdt_context* ctx, gcdt_tuning* tuning) {
     if (!ctx || !tuning) return GCDT_BAD_INPUT;
     *tuning = ctx->tuning;

@@ -74,7 +74,22 @@ def test_schedules_on_gpu_give_the_same_cdt():
     tri.close()
 
 
+@pytest.mark.gpu
+def test_autotune_keeps_a_candidate_and_the_cdt():
+    import torch
+    xy, cons = g.generate(g.GEN_SCALE, 8, 300000, 8, 40)
+    tri = g.Triangulator(max_points=len(xy), max_segments=len(cons))
+    d_xy, d_c = torch.from_numpy(xy).cuda(), torch.from_numpy(cons).cuda()
+    ref = g.canonical(tri.triangulate(d_xy, d_c)[0].cpu().numpy())
+    chosen = tri.autotune(d_xy, d_c, repeats=1)
+    assert chosen == tri.tuning() and 2 <= chosen["levels"] <= 3
+    tris = tri.triangulate(d_xy, d_c)[0].cpu().numpy()
+    assert np.array_equal(g.canonical(tris), ref)
+    tri.close()
+
+
 def test_tuning_is_validated_without_a_device():
     L = g.lib()
     assert g.STATUS[L.gcdt_set_tuning(None, None)] == "BAD_INPUT"
     assert g.STATUS[L.gcdt_get_tuning(None, None)] == "BAD_INPUT"
+    assert g.STATUS[L.gcdt_autotune(None, None, 0, None, 0, None, None, None, 1, None, None)] == "BAD_INPUT"
