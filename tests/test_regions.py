@@ -119,6 +119,27 @@ def test_kernel_bodies_on_host_equal_checker(case, order):
     assert np.all(parent[parent] == parent)
 
 
+def test_open_chains_enclose_nothing():
+    """Segments that close no loop (an open zigzag chain and a lone segment):
+    both sides of each constraint edge are one component, so every depth
+    is 0, in the checker and in the kernel bodies."""
+    rng = np.random.default_rng(12)
+    chain = np.array([[(1 << 27) * (k + 1), (1 << 28) + (1 << 26) * (k % 2)] for k in range(6)], np.int64)
+    lone = np.array([[1 << 28, 3 << 28], [3 << 28, (3 << 28) + 12345]], np.int64)
+    extra = rng.integers(1, (1 << 30) - 2, size=(5000, 2))
+    xy = np.unique(np.concatenate([chain, lone, extra]), axis=0)
+    idx = {tuple(p): i for i, p in enumerate(xy.tolist())}
+    segs = [(idx[tuple(chain[k])], idx[tuple(chain[k + 1])]) for k in range(5)]
+    segs.append((idx[tuple(lone[0])], idx[tuple(lone[1])]))
+    tris, adj, cf = _mesh(xy.astype(np.int32), np.array(segs, np.int32))
+    assert cf.any()
+    want, wmd = regions.region_depth(adj, cf)
+    assert wmd == 0 and not want.any()
+    for order in (0, 2):
+        err, depth, md, _ = _host_classify(adj, cf, order)
+        assert err == 0 and md == 0 and not depth.any()
+
+
 def test_kernel_bodies_report_bad_neighbours_on_host():
     xy, cons = g.generate(g.GEN_BATCH_INSTANCE, 3, 400)
     tris, adj, cf = _mesh(xy, cons)
