@@ -147,7 +147,8 @@ gcdt_status gcdt_get_tuning(const gcdt_context* ctx, gcdt_tuning* tuning);
    of `repeats` (1..16) device times each, keep the fastest for later solves
    on ctx and report it in *chosen (may be NULL).  The outputs hold the
    triangulation when it returns GCDT_OK; on an error the previous schedule
-   is kept.  (The batched path's counterpart is gcdt_batch_autotune.) */
+   is kept.  No counterpart in the reference, whose schedule is fixed at
+   compile time; the batched path's counterpart is gcdt_batch_autotune. */
 gcdt_status gcdt_autotune(gcdt_context* ctx, const int32_t* d_points, int32_t n,
                           const int32_t* d_segments, int32_t s, int32_t* d_tris, int32_t* d_adj,
                           uint8_t* d_cflags, int32_t repeats, gcdt_tuning* chosen, void* stream);
