@@ -79,9 +79,23 @@ __host__ __device__ __forceinline__ int body_hook(const int* adj, const uint8_t*
     return err;
 }
 
-// After all unions: point t straight at its root.
+// Root of x's tree without changing any link, or -1 if the bound ran out.
+__host__ __device__ __forceinline__ int uf_root(const int* parent, int x) {
+    for (int it = 0; it < kMaxSteps; ++it) {
+        int p = load_link(parent + x);
+        if (p == x) return x;
+        x = p;
+    }
+    return -1;
+}
+
+// After all unions: point t straight at its root.  The find here must not
+// halve paths: a halving store by another thread to parent[t] could land
+// after this thread has written the root and leave parent[t] at an inner
+// node.  With read-only finds, only thread t writes parent[t], and the trees
+// no longer change, so every entry ends at its root.
 __host__ __device__ __forceinline__ int body_compress(int t, int* parent) {
-    int r = uf_find(parent, t);
+    int r = uf_root(parent, t);
     if (r < 0) return ERR_LIMIT;
     parent[t] = r;
     return 0;

@@ -177,6 +177,24 @@ def test_gpu_classification_equals_checker(case):
 
 
 @pytest.mark.gpu
+def test_gpu_classification_at_scale_equals_host_bodies():
+    """The 10.2M-point scale mesh (20.4M triangles, 3,125 disjoint star
+    polygons): the device's concurrent union-find must label every triangle
+    as the sequential run of the same bodies does, on two calls in a row."""
+    import torch
+    xy, cons = g.generate(g.GEN_SCALE, 1)
+    tri = g.Triangulator(max_points=len(xy), max_segments=len(cons))
+    tris, adj, cf = tri.triangulate(torch.from_numpy(xy).cuda(), torch.from_numpy(cons).cuda())
+    d1, md1 = g.classify_regions(adj, cf)
+    d2, md2 = g.classify_regions(adj, cf)
+    err, want, wmd, _ = _host_classify(adj.cpu().numpy(), cf.cpu().numpy(), 0)
+    tri.close()
+    assert err == 0 and wmd == 1
+    assert md1 == md2 == 1
+    assert np.array_equal(d1.cpu().numpy(), want) and np.array_equal(d2.cpu().numpy(), want)
+
+
+@pytest.mark.gpu
 def test_gpu_classification_errors():
     import torch
     xy, cons = g.generate(g.GEN_BATCH_INSTANCE, 3, 400)
