@@ -167,9 +167,15 @@ GCDT_HD void setc(int4& v, int i, int x) {
 }
 GCDT_HD int slot_of(const int4& tv, int v) { return tv.x == v ? 0 : (tv.y == v ? 1 : 2); }
 
+// A host test build may count triangle-record accesses by defining
+// GCDT_TOUCH; the library defines nothing here.
+#ifndef GCDT_TOUCH
+#define GCDT_TOUCH()
+#endif
+
 // Vertex row (TV) and adjacency row (TA) of triangle t.
-GCDT_HD int4& tri_v(const Ctx& c, int t) { return c.tri[2 * (size_t)(unsigned)t]; }
-GCDT_HD int4& tri_a(const Ctx& c, int t) { return c.tri[2 * (size_t)(unsigned)t + 1]; }
+GCDT_HD int4& tri_v(const Ctx& c, int t) { GCDT_TOUCH(); return c.tri[2 * (size_t)(unsigned)t]; }
+GCDT_HD int4& tri_a(const Ctx& c, int t) { GCDT_TOUCH(); return c.tri[2 * (size_t)(unsigned)t + 1]; }
 
 GCDT_HD uint32_t hash32(uint32_t x) {  // bijective 32-bit mix
     x ^= x >> 16; x *= 0x7feb352dU;

@@ -14,6 +14,16 @@
 #include <vector>
 #pragma nv_diag_suppress 20011
 #pragma nv_diag_suppress 20014
+// Triangle-record accesses (vertex row or adjacency row, read or write) per
+// phase kind, counted by the host runs of the bodies.
+long long gcdt_host_touch[64];
+int gcdt_host_phase = 63;
+__host__ __device__ inline void gcdt_host_touch_one() {
+#ifndef __CUDA_ARCH__
+    ++gcdt_host_touch[gcdt_host_phase];
+#endif
+}
+#define GCDT_TOUCH() gcdt_host_touch_one()
 #include "../gcdt_b200/csrc/solver.cuh"
 
 using namespace gcdt;
@@ -45,6 +55,7 @@ void check_mesh(int kind, const Ctx& c) {
 }
 
 void host_phase(int k, const Ctx& c, long long n) {
+    gcdt_host_phase = k >= 0 && k < 63 ? k : 63;
     std::vector<int> idx((size_t)n);
     std::iota(idx.begin(), idx.end(), 0);
     if (g_order == 1) std::reverse(idx.begin(), idx.end());
@@ -63,6 +74,7 @@ void host_phase(int k, const Ctx& c, long long n) {
     } else {
         for (int i : idx) dispatch(k, c, i);
     }
+    gcdt_host_phase = 63;
     if (g_check && (k == K_FIX || k == K_FLIP_FIX)) check_mesh(k, c);
 }
 
@@ -186,4 +198,10 @@ extern "C" void host_set_limits(int rounds, int subrounds, int crounds) {
 extern "C" void host_set_tuning(int levels, int s0, int s1, int s2, int carry, int narrow_q, int narrow_act) {
     int v[7] = {levels, s0, s1, s2, carry, narrow_q, narrow_act};
     for (int k = 0; k < 7; ++k) g_tune[k] = v[k];
+}
+
+// Triangle-record accesses per phase kind since the last call (64 entries;
+// entry 63 collects accesses outside any phase), then reset.
+extern "C" void host_touch_counts(long long* out) {
+    for (int k = 0; k < 64; ++k) { out[k] = gcdt_host_touch[k]; gcdt_host_touch[k] = 0; }
 }

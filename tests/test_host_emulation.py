@@ -85,3 +85,51 @@ def test_host_emulation_matches_oracle_in_every_order(emu, name, xy, cons):
     orc, otris, _, _, _ = oracle.cdt(xy, cons)
     assert orc == 0
     assert np.array_equal(g.canonical(ref[1]), g.canonical(otris))
+
+
+def record_accesses(npts, seed=1):
+    """Triangle-record accesses (vertex or adjacency row of the 32-byte
+    record, read or write) per point and phase kind, counted by the host run
+    of the bodies on the scale workload's shape at `npts` generated points.
+    The host runs the GPU's schedule (same rounds, sub-rounds and flips), so
+    this is the kernel's record traffic if every access costs one DRAM
+    sector.  -> (n, {phase name: accesses per point})"""
+    L = ctypes.CDLL(build_host_emulation())
+    vp, i32 = ctypes.c_void_p, ctypes.c_int
+    L.host_triangulate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, i32, i32, i32]
+    L.host_touch_counts.argtypes = [vp]
+    gsz = max(2, int(round(56 * (npts / 10_000_000) ** 0.5)))
+    xy, cons = g.generate(g.GEN_SCALE, seed, npts, gsz, int(gsz * gsz * 3125 / 3136))
+    n, s, T = len(xy), len(cons), 2 * len(xy) + 2
+    out = [np.zeros((T, 3), np.int32), np.zeros((T, 3), np.int32), np.zeros(T, np.uint8)]
+    st = np.zeros(8, np.int64)
+    cnt = np.zeros(64, np.int64)
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)
+    L.host_touch_counts(p(cnt))
+    rc = L.host_triangulate(p(xy), n, p(cons), s, p(out[0]), p(out[1]), p(out[2]), p(st), 0, 2, 0)
+    L.host_touch_counts(p(cnt))
+    assert rc == 0
+    names = {}
+    for k in range(63):
+        nm = g.lib().gcdt_phase_name(k)
+        if cnt[k]:
+            names[nm.decode() if nm else "kind %d" % k] = cnt[k] / n
+    if cnt[63]:
+        names["outside phases"] = cnt[63] / n
+    return n, names
+
+
+def test_record_accesses_per_point():
+    """Traffic guard: the scale workload's shape at 200k points needs about
+    90 record accesses per point (2.9 KB at one 32-byte sector each; ncu
+    measured 2.76 KB/point of DRAM traffic at 1.02M points), 64% of them in
+    the flip passes.  A change that adds re-reads shows up here first.
+    Run with -s to print the table."""
+    n, acc = record_accesses(200000)
+    total = sum(acc.values())
+    for k, v in sorted(acc.items(), key=lambda kv: -kv[1]):
+        print("%-16s %6.1f accesses/point" % (k, v))
+    print("total %.1f accesses/point (%d points)" % (total, n))
+    assert 60 < total < 110
+    flips = acc.get("flip_check", 0) + acc.get("flip_do", 0) + acc.get("flip_fix", 0)
+    assert 0.5 < flips / total < 0.75
