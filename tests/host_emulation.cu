@@ -17,6 +17,7 @@
 // Triangle-record accesses (vertex row or adjacency row, read or write) per
 // phase kind, counted by the host runs of the bodies.
 long long gcdt_host_touch[64];
+long long gcdt_host_items[64];
 int gcdt_host_phase = 63;
 __host__ __device__ inline void gcdt_host_touch_one() {
 #ifndef __CUDA_ARCH__
@@ -56,6 +57,7 @@ void check_mesh(int kind, const Ctx& c) {
 
 void host_phase(int k, const Ctx& c, long long n) {
     gcdt_host_phase = k >= 0 && k < 63 ? k : 63;
+    gcdt_host_items[gcdt_host_phase] += n;
     std::vector<int> idx((size_t)n);
     std::iota(idx.begin(), idx.end(), 0);
     if (g_order == 1) std::reverse(idx.begin(), idx.end());
@@ -201,7 +203,13 @@ extern "C" void host_set_tuning(int levels, int s0, int s1, int s2, int carry, i
 }
 
 // Triangle-record accesses per phase kind since the last call (64 entries;
-// entry 63 collects accesses outside any phase), then reset.
-extern "C" void host_touch_counts(long long* out) {
-    for (int k = 0; k < 64; ++k) { out[k] = gcdt_host_touch[k]; gcdt_host_touch[k] = 0; }
+// entry 63 collects accesses outside any phase) and, if items is not null,
+// the items each phase kind ran over; then reset both.
+extern "C" void host_touch_counts(long long* out, long long* items) {
+    for (int k = 0; k < 64; ++k) {
+        out[k] = gcdt_host_touch[k];
+        if (items) items[k] = gcdt_host_items[k];
+        gcdt_host_touch[k] = 0;
+        gcdt_host_items[k] = 0;
+    }
 }

@@ -93,30 +93,34 @@ def record_accesses(npts, seed=1):
     of the bodies on the scale workload's shape at `npts` generated points.
     The host runs the GPU's schedule (same rounds, sub-rounds and flips), so
     this is the kernel's record traffic if every access costs one DRAM
-    sector.  -> (n, {phase name: accesses per point})"""
+    sector.  -> (n, {phase name: accesses per point},
+    {phase name: items the phase ran over, per point})"""
     L = ctypes.CDLL(build_host_emulation())
     vp, i32 = ctypes.c_void_p, ctypes.c_int
     L.host_triangulate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, i32, i32, i32]
-    L.host_touch_counts.argtypes = [vp]
+    L.host_touch_counts.argtypes = [vp, vp]
     gsz = max(2, int(round(56 * (npts / 10_000_000) ** 0.5)))
     xy, cons = g.generate(g.GEN_SCALE, seed, npts, gsz, int(gsz * gsz * 3125 / 3136))
     n, s, T = len(xy), len(cons), 2 * len(xy) + 2
     out = [np.zeros((T, 3), np.int32), np.zeros((T, 3), np.int32), np.zeros(T, np.uint8)]
     st = np.zeros(8, np.int64)
     cnt = np.zeros(64, np.int64)
+    items = np.zeros(64, np.int64)
     p = lambda a: ctypes.c_void_p(a.ctypes.data)
-    L.host_touch_counts(p(cnt))
+    L.host_touch_counts(p(cnt), p(items))
     rc = L.host_triangulate(p(xy), n, p(cons), s, p(out[0]), p(out[1]), p(out[2]), p(st), 0, 2, 0)
-    L.host_touch_counts(p(cnt))
+    L.host_touch_counts(p(cnt), p(items))
     assert rc == 0
-    names = {}
+    names, per_item = {}, {}
     for k in range(63):
         nm = g.lib().gcdt_phase_name(k)
         if cnt[k]:
-            names[nm.decode() if nm else "kind %d" % k] = cnt[k] / n
+            key = nm.decode() if nm else "kind %d" % k
+            names[key] = cnt[k] / n
+            per_item[key] = items[k] / n
     if cnt[63]:
         names["outside phases"] = cnt[63] / n
-    return n, names
+    return n, names, per_item
 
 
 def test_record_accesses_per_point():
@@ -125,10 +129,12 @@ def test_record_accesses_per_point():
     measured 2.76 KB/point of DRAM traffic at 1.02M points), 64% of them in
     the flip passes.  A change that adds re-reads shows up here first.
     Run with -s to print the table."""
-    n, acc = record_accesses(200000)
+    n, acc, items = record_accesses(200000)
     total = sum(acc.values())
     for k, v in sorted(acc.items(), key=lambda kv: -kv[1]):
-        print("%-16s %6.1f accesses/point" % (k, v))
+        it = items.get(k, 0)
+        print("%-16s %6.1f accesses/point  %6.2f items/point  %5.1f accesses/item" % (
+            k, v, it, v / it if it else 0))
     print("total %.1f accesses/point (%d points)" % (total, n))
     assert 60 < total < 110
     flips = acc.get("flip_check", 0) + acc.get("flip_do", 0) + acc.get("flip_fix", 0)
