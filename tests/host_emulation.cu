@@ -18,6 +18,9 @@
 // phase kind, counted by the host runs of the bodies.
 long long gcdt_host_touch[64];
 long long gcdt_host_items[64];
+// Flip-queue outcomes: entries checked, entries with a candidate edge,
+// distinct candidate edges, flips.
+long long g_fq[4];
 int gcdt_host_phase = 63;
 __host__ __device__ inline void gcdt_host_touch_one() {
 #ifndef __CUDA_ARCH__
@@ -77,6 +80,19 @@ void host_phase(int k, const Ctx& c, long long n) {
         for (int i : idx) dispatch(k, c, i);
     }
     gcdt_host_phase = 63;
+    if (k == K_FLIP_CHECK) {
+        std::vector<long long> edges;
+        for (long long i = 0; i < n; ++i) {
+            int2 cd = c.cand[i];
+            if (cd.x < 0) continue;
+            edges.push_back(cd.x < cd.y ? cd.x : cd.y);
+        }
+        std::sort(edges.begin(), edges.end());
+        g_fq[0] += n;
+        g_fq[1] += (long long)edges.size();
+        g_fq[2] += (long long)(std::unique(edges.begin(), edges.end()) - edges.begin());
+    }
+    if (k == K_FLIP_DO) g_fq[3] += (long long)(c.cnt->cur_flip - c.base_flip);
     if (g_check && (k == K_FIX || k == K_FLIP_FIX)) check_mesh(k, c);
 }
 
@@ -212,4 +228,10 @@ extern "C" void host_touch_counts(long long* out, long long* items) {
         gcdt_host_touch[k] = 0;
         gcdt_host_items[k] = 0;
     }
+}
+
+// Flip-queue outcomes since the last call: entries checked, entries that
+// found a non-locally-Delaunay edge, distinct such edges, flips; then reset.
+extern "C" void host_flip_outcomes(long long* out) {
+    for (int k = 0; k < 4; ++k) { out[k] = g_fq[k]; g_fq[k] = 0; }
 }

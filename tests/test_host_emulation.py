@@ -94,11 +94,13 @@ def record_accesses(npts, seed=1):
     The host runs the GPU's schedule (same rounds, sub-rounds and flips), so
     this is the kernel's record traffic if every access costs one DRAM
     sector.  -> (n, {phase name: accesses per point},
-    {phase name: items the phase ran over, per point})"""
+    {phase name: items the phase ran over, per point}); the flip-queue
+    outcomes per point are left in record_accesses.flip_outcomes."""
     L = ctypes.CDLL(build_host_emulation())
     vp, i32 = ctypes.c_void_p, ctypes.c_int
     L.host_triangulate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, i32, i32, i32]
     L.host_touch_counts.argtypes = [vp, vp]
+    L.host_flip_outcomes.argtypes = [vp]
     gsz = max(2, int(round(56 * (npts / 10_000_000) ** 0.5)))
     xy, cons = g.generate(g.GEN_SCALE, seed, npts, gsz, int(gsz * gsz * 3125 / 3136))
     n, s, T = len(xy), len(cons), 2 * len(xy) + 2
@@ -106,10 +108,13 @@ def record_accesses(npts, seed=1):
     st = np.zeros(8, np.int64)
     cnt = np.zeros(64, np.int64)
     items = np.zeros(64, np.int64)
+    fo = np.zeros(4, np.int64)
     p = lambda a: ctypes.c_void_p(a.ctypes.data)
     L.host_touch_counts(p(cnt), p(items))
+    L.host_flip_outcomes(p(fo))
     rc = L.host_triangulate(p(xy), n, p(cons), s, p(out[0]), p(out[1]), p(out[2]), p(st), 0, 2, 0)
     L.host_touch_counts(p(cnt), p(items))
+    L.host_flip_outcomes(p(fo))
     assert rc == 0
     names, per_item = {}, {}
     for k in range(63):
@@ -120,6 +125,8 @@ def record_accesses(npts, seed=1):
             per_item[key] = items[k] / n
     if cnt[63]:
         names["outside phases"] = cnt[63] / n
+    record_accesses.flip_outcomes = {"entries": fo[0] / n, "with_candidate": fo[1] / n,
+                                     "distinct_candidates": fo[2] / n, "flips": fo[3] / n}
     return n, names, per_item
 
 
@@ -136,6 +143,10 @@ def test_record_accesses_per_point():
         print("%-16s %6.1f accesses/point  %6.2f items/point  %5.1f accesses/item" % (
             k, v, it, v / it if it else 0))
     print("total %.1f accesses/point (%d points)" % (total, n))
+    fo = record_accesses.flip_outcomes
+    print("flip queue per point: %.2f entries, %.2f with a candidate edge, %.2f distinct candidate "
+          "edges, %.2f flips" % (fo["entries"], fo["with_candidate"], fo["distinct_candidates"], fo["flips"]))
     assert 60 < total < 110
+    assert fo["flips"] <= fo["distinct_candidates"] <= fo["with_candidate"] <= fo["entries"]
     flips = acc.get("flip_check", 0) + acc.get("flip_do", 0) + acc.get("flip_fix", 0)
     assert 0.5 < flips / total < 0.75
