@@ -649,8 +649,12 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
 #ifdef GCDT_FLIP_ONE_SIDE
         int m0 = resolve_split_edge_dup(c, t, 0), m1 = resolve_split_edge_dup(c, T1, 1);
         int m2 = resolve_split_edge_dup(c, T2, 2);
-        int* qn = c.queue_next + append_slots(&c.cnt->cur_q, c.base_q, 3);
-        qn[0] = qentry(t, 1 & ~m0); qn[1] = qentry(T1, 2 & ~m1); qn[2] = qentry(T2, 4 & ~m2);
+        // children whose only old edge the other side tests are not queued
+        const int keep = !m0 + !m1 + !m2;
+        int* qn = c.queue_next + append_slots(&c.cnt->cur_q, c.base_q, keep);
+        if (!m0) *qn++ = qentry(t, 1);
+        if (!m1) *qn++ = qentry(T1, 2);
+        if (!m2) *qn++ = qentry(T2, 4);
 #else
         resolve_split_edge(c, t, 0);
         resolve_split_edge(c, T1, 1);

@@ -206,3 +206,4 @@ def test_one_sided_edge_tests_cut_duplicate_candidates():
     dup1 = f1["with_candidate"] - f1["distinct_candidates"]
     assert dup1 < 0.4 * dup0
     assert a1["flip_check"] < 0.9 * a0["flip_check"]
+    assert f1["entries"] < 0.95 * f0["entries"]
