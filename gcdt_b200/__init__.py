@@ -65,6 +65,12 @@ class Stats(ctypes.Structure):
 
 
 def lib_path():
+    """The CUDA library: libgcdt_b200.so next to this file, or the build
+    variant named by GCDT_B200_LIB (a path, or a variant name such as
+    "oneside" for libgcdt_b200_oneside.so; see build.VARIANTS)."""
+    v = os.environ.get("GCDT_B200_LIB")
+    if v:
+        return v if os.sep in v else os.path.join(_HERE, "libgcdt_b200_%s.so" % v)
     return os.path.join(_HERE, "libgcdt_b200.so")
 
 
@@ -75,7 +81,7 @@ def lib():
         return _LIB
     path = lib_path()
     if not os.path.exists(path):
-        raise ImportError("libgcdt_b200.so is missing; build it with `python -m gcdt_b200.build`")
+        raise ImportError("%s is missing; build it with `python -m gcdt_b200.build`" % path)
     L = ctypes.CDLL(path)
     vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
     L.gcdt_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, i64, i64]

@@ -56,11 +56,18 @@ def _deps(*names):
     return files
 
 
-def build(force=False, verbose=False, ptxas_verbose=False):
-    out = os.path.join(HERE, "libgcdt_b200.so")
+# Compile-time variants of the solver bodies, built next to the default
+# library for measurement (GCDT_B200_LIB selects one at import):
+#   oneside  GCDT_FLIP_ONE_SIDE: an edge of two triangles split in the same
+#            round, or flipped in the same sub-round, is tested from one side.
+VARIANTS = {"oneside": ["-DGCDT_FLIP_ONE_SIDE"]}
+
+
+def build(force=False, verbose=False, ptxas_verbose=False, variant=None):
+    out = os.path.join(HERE, "libgcdt_b200.so" if not variant else "libgcdt_b200_%s.so" % variant)
     srcs = ["gcdt.cu", "batch.cu", "server.cu", "surface.cu", "reorder.cu", "regions.cu", "io.cpp"]
     if force or _stale(out, _deps(*srcs)):
-        flags = list(NVCC_FLAGS)
+        flags = list(NVCC_FLAGS) + (VARIANTS[variant] if variant else [])
         if ptxas_verbose:
             flags += ["-Xptxas", "-v"]
         r = _run([_nvcc()] + flags + ["-o", out] + [os.path.join(CSRC, s) for s in srcs], verbose)
@@ -74,4 +81,5 @@ def build(force=False, verbose=False, ptxas_verbose=False):
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True, ptxas_verbose="--ptxas" in sys.argv)
+    var = sys.argv[sys.argv.index("--variant") + 1] if "--variant" in sys.argv else None
+    build(force="--force" in sys.argv, verbose=True, ptxas_verbose="--ptxas" in sys.argv, variant=var)

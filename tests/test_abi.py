@@ -88,3 +88,22 @@ def test_canonical_is_rotation_invariant():
     r = np.array([[4, 6, 5], [1, 2, 3]])
     assert np.array_equal(g.canonical(t), g.canonical(r))
     assert not np.array_equal(g.canonical(t), g.canonical(t[:, ::-1]))
+
+
+def test_variant_library_selection(monkeypatch):
+    """GCDT_B200_LIB names a build variant (or a path); unset, the default
+    library is used.  A missing variant fails loudly at load."""
+    import importlib
+    monkeypatch.delenv("GCDT_B200_LIB", raising=False)
+    assert g.lib_path().endswith(os.path.join("gcdt_b200", "libgcdt_b200.so"))
+    monkeypatch.setenv("GCDT_B200_LIB", "oneside")
+    assert g.lib_path().endswith(os.path.join("gcdt_b200", "libgcdt_b200_oneside.so"))
+    monkeypatch.setenv("GCDT_B200_LIB", "/nonexistent/libx.so")
+    assert g.lib_path() == "/nonexistent/libx.so"
+    saved = g._LIB
+    try:
+        g._LIB = None
+        with pytest.raises(ImportError):
+            g.lib()
+    finally:
+        g._LIB = saved
