@@ -4,7 +4,6 @@
 #include <cstdio>
 #include <cstring>
 #include <cstddef>
-#include <mutex>
 #include <new>
 
 #include "solver.cuh"
@@ -471,10 +470,13 @@ extern "C" gcdt_status gcdt_probe_barrier(int device, int32_t blocks, int32_t ab
 // module, so every GPU that loads the library holds it until the process
 // exits.
 //
-// Set-up: the first call on each device (made with that device current)
-// looks the array's device address up with cudaGetSymbolAddress; later calls
-// on that device reuse it.  Make that first call before any stream capture
-// begins on the device.
+// Set-up: every call looks the array's device address up with
+// cudaGetSymbolAddress on the device that is current when it is called (the
+// lookup is a host-side table read, so it costs little), and checks the
+// result.  Nothing is cached across calls, so the address stays right after
+// a cudaDeviceReset reloads the module.  Since every call does this set-up,
+// make every call before any stream capture begins on the device.  The call
+// returns once the solve has finished (it reads the solve's counters back).
 //
 // Limits and sharing: a problem whose workspace (gcdt_workspace_bytes(n, s))
 // exceeds GCDT_NOALLOC_WORKSPACE_BYTES is rejected with GCDT_OOM before any
@@ -487,9 +489,6 @@ extern "C" gcdt_status gcdt_probe_barrier(int device, int32_t blocks, int32_t ab
 namespace {
 constexpr size_t kNoAllocBytes = GCDT_NOALLOC_WORKSPACE_BYTES;
 __device__ __align__(256) unsigned char g_noalloc_workspace[kNoAllocBytes];
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-char* g_noalloc_base[kNoAllocMaxDevices] = {};
 }  // namespace
 
 extern "C" gcdt_status gcdt_triangulate_noalloc(const int32_t* d_points, int32_t n,
@@ -500,25 +499,15 @@ extern "C" gcdt_status gcdt_triangulate_noalloc(const int32_t* d_points, int32_t
         return GCDT_BAD_INPUT;
     Plan plan = make_plan(n, s, sort_temp_bytes(n));
     if (plan.L.total > kNoAllocBytes) return GCDT_OOM;
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    // The device address of the array on the current device.  In host code
+    // g_noalloc_workspace names a host-side stand-in, never a device address.
+    void* sym = nullptr;
+    cudaError_t se = cudaGetSymbolAddress(&sym, g_noalloc_workspace);
+    if (se != cudaSuccess || !sym) {
         cudaGetLastError();
         return GCDT_CUDA_ERROR;
     }
-    char* base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_base[dev]) {
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_workspace);
-            if (e != cudaSuccess || !p) {
-                cudaGetLastError();
-                return GCDT_CUDA_ERROR;
-            }
-            g_noalloc_base[dev] = static_cast<char*>(p);
-        }
-        base = g_noalloc_base[dev];
-    }
+    char* base = static_cast<char*>(sym);
     Ctx c = bind_ctx(base, plan);
     c.in_xy = reinterpret_cast<const int2*>(d_points);
     c.in_cons = reinterpret_cast<const int2*>(d_segments);
@@ -535,7 +524,10 @@ extern "C" gcdt_status gcdt_triangulate_noalloc(const int32_t* d_points, int32_t
     SolveStats st;
     int bits = run_solve(bk, c, st);
     bk.note(cudaStreamSynchronize(bk.st));
-    if (bk.err != cudaSuccess) bits |= ST_CUDA;
+    if (bk.err != cudaSuccess) {
+        bits |= ST_CUDA;
+        cudaGetLastError();   // clear a launch error so the caller's next check does not see it
+    }
     gcdt_status rc = map_status(bits);
     if (rc == GCDT_OK && n_tris) *n_tris = 2 * n + 2;
     return rc;

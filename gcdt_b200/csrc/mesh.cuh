@@ -1,6 +1,7 @@
 // mesh.cuh -- data layout and per-element bodies of every kernel of the
 // CDT path.  The bodies are __host__ __device__ so that the same code is
-// what the CUDA kernels (kernels.cu) run, one body call per thread.
+// what the CUDA kernels (gcdt.cu, batch.cu) run, one body call per thread,
+// and what the host test harness runs on the CPU.
 //
 // Layout in HBM (structure of arrays, one row per point or triangle):
 //   P[v]      int2   point v in Morton-sorted order; corners at N..N+3

@@ -1,5 +1,6 @@
 // solver.cuh -- round structure of one CDT solve, written once against a
-// launch backend (kernels.cu supplies the CUDA one).
+// launch backend (gcdt.cu supplies the CUDA one: the persistent stage
+// kernel with its grid executor from exec.cuh).
 //
 // Phases (reference stage it replaces, yingtix/gCDT):
 //   0  Morton keys, radix sort, gather: points in spatial order

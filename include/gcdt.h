@@ -337,9 +337,11 @@ int gcdt_text_save(const char* path, const int32_t* points_xy, int64_t n_points,
    latency-bound loops that cannot pay for cudaMalloc/cudaFree (which may
    synchronize the device).  Scratch lives in one static device array of
    GCDT_NOALLOC_WORKSPACE_BYTES inside this library, held by every GPU that
-   loads it until the process exits.  The first call on a device (with that
-   device current) looks up the array's address; make that call before any
-   stream capture starts.  Problems needing more workspace than the array
+   loads it until the process exits.  Every call looks up the array's
+   address on the current device (nothing is cached, so a device reset does
+   not leave a stale address); as that is the call's set-up, make every call
+   before any stream capture starts on the device.  The call returns once the
+   solve has finished.  Problems needing more workspace than the array
    (gcdt_workspace_bytes(n, s) > GCDT_NOALLOC_WORKSPACE_BYTES, about 100,000
    points) return GCDT_OOM without touching the device.  Calls share the
    array: calls that overlap on the GPU race and corrupt each other, so

@@ -16,7 +16,7 @@
 #   5. kernel.cu                `return;` at the end of main -> `return 0;`
 #   6. utils.cu                 drop six duplicate RKERNEL explicit instantiations
 # kernel.cu is compiled with -Dmain=gcdt_ref_unused_main; the harness
-# supplies main.
+# supplies main.  With --if-present, a missing source tree is not an error.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF="${GCDT_REFERENCE_DIR:-/root/reference}"
@@ -25,6 +25,9 @@ WORK="$(mktemp -d /tmp/gcdt_ref_src.XXXXXX)"
 trap 'rm -rf "$WORK"' EXIT
 
 if [ ! -f "$REF/kernel.cu" ]; then
+    if [ "${1:-}" = "--if-present" ]; then
+        exit 0      # nothing to build where the sources are absent (the GPU side uses the built file)
+    fi
     echo "reference sources not found at $REF" >&2
     exit 1
 fi

@@ -105,3 +105,29 @@ def test_full_scale_workload_properties():
     tris2, adj2, cf2 = tri.triangulate_host(xy, cons)
     assert np.array_equal(tris, tris2) and np.array_equal(adj, adj2) and np.array_equal(cf, cf2)
     tri.close()
+    # the oracle's own CDT of the same 10.2M + 200k instance (about 8 s on
+    # one core): canonical triangle set with the flags rotated along
+    rc, otris, _, ocf, _ = oracle.cdt(xy, cons)
+    assert rc == 0
+    assert np.array_equal(canonical_with_flags(tris, cf), canonical_with_flags(otris, ocf))
+
+
+def test_full_size_lattice_config():
+    """The degenerate lattice workload at full size: a 2048 x 2048 lattice of
+    spacing 2^14 offset by (2^14, 2^14), N = 4,194,304, with 20,000 unit
+    constraint segments on the sides of disjoint lattice rectangles.  Every
+    empty circle through four lattice neighbours is a tie, which the shared
+    symbolic perturbation resolves; the reference keeps whatever diagonal it
+    had (strict inCircle > 0, kernel.cu:2218-2219), so its count 2N+2 and
+    the exact validator are what it pins, and the oracle pins the set."""
+    xy, cons = g.generate(g.GEN_LATTICE, 1)
+    assert len(xy) == 2048 * 2048 and len(cons) == 20000
+    tri = g.Triangulator(max_points=len(xy), max_segments=len(cons))
+    tris, adj, cf = tri.triangulate_host(xy, cons)
+    tri.close()
+    assert len(tris) == 2 * len(xy) + 2
+    ok, msg = oracle.validate(xy, cons, tris, adj, cf)
+    assert ok, msg
+    rc, otris, _, ocf, _ = oracle.cdt(xy, cons)
+    assert rc == 0
+    assert np.array_equal(canonical_with_flags(tris, cf), canonical_with_flags(otris, ocf))

@@ -51,8 +51,8 @@ def _run_noalloc(xy, cons, poison):
 def test_noalloc_equals_context_entry_point_twice_in_a_row():
     inputs = [g.generate(g.GEN_SMALL, 1),                     # 100,512 points + 512 segments
               g.generate(g.GEN_BATCH_INSTANCE, 3, 20000)]     # a different, smaller instance
-    for xy, _ in inputs:
-        assert g.workspace_bytes(len(xy), 512) <= (32 << 20)
+    for xy, cons in inputs:
+        assert g.workspace_bytes(len(xy), len(cons)) <= (32 << 20)
     tri = g.Triangulator(max_points=max(len(x) for x, _ in inputs),
                          max_segments=max(len(c) for _, c in inputs))
     expected = [tri.triangulate_host(xy, cons) for xy, cons in inputs]
