@@ -14,13 +14,21 @@ inputs double-buffered over two contexts and two streams
 (gcdt_triangulate_async: solves in order, copies overlapped); e2e.serial is
 the one-step-at-a-time figure.
 
+At N = 1 the default run also reports, after the timed region: the exact
+validation of the timed output, the single-threaded CPU oracle on the same
+instance (`cpu_baseline`), the reference's own CUDA build on the same
+instance and on its own default input (`reference_cuda`), the degenerate
+lattice workload (`lattice`), the 4,096-instance batched workload
+(`batched`) and the 20,000-request serving stream (`serving`).
+`--headline-only` skips them.
+
 N > 1 runs independent replicas, one per rank (the path has no data-parallel
 exchange: a single triangulation stays on one GPU), so scaling is weak.
 
 --impl reference times the CPU path (the sequential exact oracle, the
 reference having no host implementation of this path) on every host thread
-at once, each thread solving its own bounded sample of the same workload
-shape.
+at once, each thread solving its own seeded full-size instance of the same
+workload.
 """
 import argparse
 import json
@@ -39,7 +47,6 @@ sys.path.insert(0, ROOT)
 METRIC = "CDT Mpts/s at 10M pts+200k segs"
 UNIT = "Mpts/s"
 WORKLOAD = "plain CDT at scale: 10M Gaussian-mixture/uniform int32 points in [1,2^30-2]^2 + 3,125 star polygons (200,000 segments)"
-CPU_SAMPLE_POINTS = 2_000_000   # config-shaped sample for the CPU legs (18x18 polygon grid, 632 polygons)
 # DRAM bytes (read + write) of the stage kernel per point, from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the same workload shape at
 # 1,020,608 points: 1,890,871,040 + 921,974,272 bytes.  Reported per solve as
@@ -166,66 +173,68 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def cpu_oracle_sample(seed=1, repeat=1):
-    """Time the single-threaded oracle on a config-shaped sample."""
-    import gcdt_b200 as g
+def workload_config(n, s):
+    """The `config` object of both arms: the workload and its sizes."""
+    return {"workload": WORKLOAD, "n_points": int(n), "n_segments": int(s), "n_triangles": 2 * int(n) + 2}
+
+
+def cpu_oracle_full(xy, cons):
+    """Time the single-threaded oracle on the given full instance (the
+    headline instance itself); returns (Mpts/s, seconds)."""
     from oracle import oracle
-    xy, cons = g.generate(g.GEN_SCALE, seed, CPU_SAMPLE_POINTS, 18, 316)
-    times = []
-    for _ in range(repeat):
-        t0 = time.perf_counter()
-        rc, tris, _, _, _ = oracle.cdt(xy, cons)
-        times.append(time.perf_counter() - t0)
-        if rc != 0:
-            raise RuntimeError("oracle failed on the CPU sample: %d" % rc)
-    t = min(times)
-    sample = "%d points + %d segments (scale workload shape, 18x18 polygon grid), best of %d" % (
-        len(xy), len(cons), repeat)
-    return len(xy) / t / 1e6, sample, len(xy), t
+    t0 = time.perf_counter()
+    rc = oracle.cdt(xy, cons)[0]
+    t = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError("oracle failed on the headline instance: %d" % rc)
+    return len(xy) / t / 1e6, t
 
 
-# Peak resident bytes of one oracle solve of the CPU sample (its 2.02M points,
-# the mesh, the Morton keys and the outputs measured at ~210 MB), with margin.
-CPU_SAMPLE_BYTES = 400 << 20
+# Peak resident bytes of one oracle solve of a full scale instance (measured
+# at ~1.0 GB above the process base, plus the 83 MB input and the generator's
+# transient buffers), with margin.
+CPU_INSTANCE_BYTES = 2 << 30
 
 
 def cpu_threads():
     """Host threads for the CPU leg: every core this process may run on,
-    fewer if half the available memory cannot hold one sample per thread."""
+    fewer if half the available memory cannot hold one instance per thread."""
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     try:
         with open("/proc/meminfo") as f:
             avail = next(int(l.split()[1]) * 1024 for l in f if l.startswith("MemAvailable:"))
-        cores = min(cores, max(1, avail // 2 // CPU_SAMPLE_BYTES))
+        cores = min(cores, max(1, avail // 2 // CPU_INSTANCE_BYTES))
     except Exception:
         pass
     return max(1, cores)
 
 
-def cpu_oracle_parallel(threads, steps, points=CPU_SAMPLE_POINTS):
+def cpu_oracle_parallel(threads, steps, scale_points=0):
     """Time the sequential oracle on every host thread at once, each thread
-    solving its own seeded config-shaped sample; one step = all threads'
-    solves, timed from the common start to the last finish.  Returns the
-    per-step (Mpts/s, seconds) and the sample description."""
+    solving its own seeded full-size instance of the scale workload (thread
+    i: seed 1 + i; thread 0's instance is the headline instance).  One step =
+    all threads' solves, timed from the common start to the last finish.
+    Returns the per-step (Mpts/s, seconds), the description and the headline
+    instance's sizes.  `scale_points` (tests only) shrinks the instances to
+    reduced copies of the same shape."""
     from concurrent.futures import ThreadPoolExecutor
-    import gcdt_b200 as g
     from oracle import oracle
     with ThreadPoolExecutor(threads) as ex:
-        samples = list(ex.map(lambda i: g.generate(g.GEN_SCALE, 1 + i, points, 18, 316),
-                              range(threads)))
-        total = sum(len(xy) for xy, _ in samples)
+        inst = list(ex.map(lambda i: replica_workload(i, scale_points), range(threads)))
+        total = sum(len(xy) for xy, _ in inst)
         out = []
         for _ in range(steps):
             t0 = time.perf_counter()
-            rcs = list(ex.map(lambda s: oracle.cdt(*s)[0], samples))
+            rcs = list(ex.map(lambda s: oracle.cdt(*s)[0], inst))
             t = time.perf_counter() - t0
             if any(rcs):
-                raise RuntimeError("oracle failed on a CPU sample: %r" % (rcs,))
+                raise RuntimeError("oracle failed on an instance: %r" % (rcs,))
             out.append((total / t / 1e6, t))
-    desc = ("%d concurrent samples (one per thread) of ~%d points + %d segments each, %d points in all "
-            "(scale workload shape, 18x18 polygon grid, seeds 1..%d)" % (
-                threads, len(samples[0][0]), len(samples[0][1]), total, threads))
-    return out, desc
+    desc = ("%d concurrent %s instances of the scale workload (one per thread, seeds 1..%d; "
+            "seed 1 is the headline instance), %d points in all" % (
+                threads, "full-size" if not scale_points else "reduced (%d generated points)" % scale_points,
+                threads, total))
+    return out, desc, (len(inst[0][0]), len(inst[0][1]))
 
 
 def run_reference(args):
@@ -233,7 +242,7 @@ def run_reference(args):
     if rank != 0:
         return
     threads = cpu_threads()
-    runs, sample = cpu_oracle_parallel(threads, args.warmup + args.steps)
+    runs, sample, (n0, s0) = cpu_oracle_parallel(threads, args.warmup + args.steps)
     vals = runs[args.warmup:]
     value = statistics.median([v for v, _ in vals])
     ms = statistics.median([t for _, t in vals]) * 1e3
@@ -242,8 +251,8 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "i64/i128 exact predicates on i32 coordinates", "data": "synthetic",
-        "config": {"workload": WORKLOAD + " -- CPU leg: bounded samples per step",
-                   "parallelism": "%d host threads, one independent sample each" % threads},
+        "config": workload_config(n0, s0),
+        "parallelism": "%d host threads, one independent full-size instance each" % threads,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample + "; sequential exact incremental CDT (oracle/cdt_oracle.c) per thread; "
                                    "the reference has no host implementation of this path"},
@@ -373,9 +382,11 @@ def run_ours(args):
     h2d = xy.nbytes + cons.nbytes
     d2h = T * 12 * 2 + T
 
-    # sanity: the timed output is a valid CDT
+    # the timed output is checked by the exact validator (orientation,
+    # adjacency, box hull, Euler count, every constraint present and
+    # flagged, every unconstrained edge locally Delaunay)
     valid = None
-    if rank == 0 and args.validate:
+    if rank == 0 and not args.no_validate:
         from oracle import oracle
         ok, msg = oracle.validate(xy, cons, h_out[0].numpy(), h_out[1].numpy(), h_out[2].numpy())
         valid = ok if ok else msg
@@ -383,24 +394,30 @@ def run_ours(args):
     peak, peak_kind = peaks()
     b_alg = 8 * n + 8 * s + T * 25
     achieved = b_alg / (ms_local * 1e-3) / 1e9
-    line = None
+    extras = {}
+    if rank == 0 and world == 1 and not args.headline_only:
+        # measured after the timed region, on the same box and process
+        extras = run_extras(args, tri, xy, cons, dev)
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            v, sample, _, _ = cpu_oracle_sample(seed=1, repeat=args.cpu_repeat)
-            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                   "sample": sample + "; single-threaded exact incremental CDT (oracle/cdt_oracle.c)"}
+            v, t_cpu = cpu_oracle_full(xy, cons)
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "seconds": t_cpu,
+                   "sample": "the headline instance itself (%d points + %d segments), one solve; "
+                             "single-threaded exact incremental CDT (oracle/cdt_oracle.c)" % (n, s)}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "i64/i128 exact predicates on i32 coordinates (f64 filter)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD if not args.scale_points else "PROFILING ONLY, reduced: %d generated points" % args.scale_points,
-                       "n_points": n, "n_segments": s, "n_triangles": T,
-                       "parallelism": "replicas (one independent triangulation per GPU)" if world > 1 else "single GPU",
-                       "schedule": tri.tuning(),
-                       "l2": "256 MB buffer written between timed steps; working set ~2 GB"},
+            "config": workload_config(n, s) if not args.scale_points else
+                      {"workload": "PROFILING ONLY, reduced: %d generated points" % args.scale_points,
+                       "n_points": n, "n_segments": s, "n_triangles": T},
+            "parallelism": "replicas (one independent triangulation per GPU)" if world > 1 else "single GPU",
+            "schedule": tri.tuning(),
+            "library": os.path.basename(g.lib_path()),
+            "l2": "256 MB buffer written between timed steps; working set ~2 GB",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": args.traffic if args.traffic is not None else DRAM_BYTES_PER_POINT * n,
@@ -423,9 +440,119 @@ def run_ours(args):
             "step_ms": step_ms,
             "validated": valid,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     tri.close()
     dist_done(world)
+
+
+def _guarded(name, fn, errors):
+    """Run one extra measurement; a failure is reported in the line instead
+    of ending the run."""
+    t0 = time.perf_counter()
+    try:
+        r = fn()
+    except Exception as e:  # noqa: BLE001 -- reported, not hidden
+        errors[name] = "%s: %s" % (type(e).__name__, e)
+        return None
+    if isinstance(r, dict):
+        r["wall_s"] = round(time.perf_counter() - t0, 2)
+    return r
+
+
+def run_extras(args, tri, xy, cons, dev):
+    """The other workloads and comparison points, measured after the headline
+    timed region: the reference's CUDA build, the lattice, batched and serving."""
+    errors = {}
+    out = {}
+    out["reference_cuda"] = _guarded("reference_cuda", lambda: measure_reference_cuda(args, xy, cons, dev), errors)
+    out["lattice"] = _guarded("lattice", lambda: measure_lattice(args, dev), errors)
+    out["batched"] = _guarded("batched", lambda: measure_batched(args, dev, steps=5, warmup=3,
+                                                                  validate=True), errors)
+    out["serving"] = _guarded("serving", lambda: measure_serving(args), errors)
+    if errors:
+        out["extras_errors"] = errors
+    return out
+
+
+def _time_solves(tri, d_xy, d_cons, steps, warmup, dev, out=None):
+    """Median CUDA-event ms of `steps` device-resident solves after `warmup`,
+    with the L2 flushed before each."""
+    import torch
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        r = tri.triangulate(d_xy, d_cons, out=out)
+    ms = []
+    for k in range(steps):
+        flush.fill_(k & 255)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = tri.triangulate(d_xy, d_cons, out=out)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    del flush
+    return statistics.median(ms), r
+
+
+def measure_reference_cuda(args, xy, cons, dev):
+    """The reference's own CUDA pipeline (yingtix/gCDT built for sm_100a from
+    its sources, run as a separate process that replays its driver's stage
+    sequence, kernel.cu:5398-5443) on (i) the headline instance and (ii) its
+    own default input, 9M uniform points (kernel.cu:43-58), where its output
+    is complete; ours is timed on the same 9M input beside it.  The
+    reference's time is its outer cudaEvent pair around the stages, inputs
+    on the device."""
+    import torch
+    import gcdt_b200 as g
+    from oracle import reference
+    if not reference.available():
+        return {"unavailable": "oracle/_ref/gcdt_ref not built (reference sources absent at build time)"}
+    os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")   # no lazy module loads inside its timed stages
+    res = {"kind": "reference CUDA build, one solve per process, stage timer = outer cudaEvent pair"}
+    r = reference.run(xy, cons, repeat=1, timeout=300)
+    res["headline"] = {
+        "ref_ms": r["event_ms"], "ref_sum_time_ms": r["sum_time"], "ref_triangles": int(len(r["tris"])),
+        "ref_ignored_segments": r["ignored"][-1] if r["ignored"] else None,
+        "ref_final_mark": r["marks"][-1] if r["marks"] else None,
+        "ours_ms": None, "n_points": len(xy), "n_segments": len(cons),
+        "ref_mpts_per_s": len(xy) / (r["event_ms"] * 1e-3) / 1e6}
+    uxy, _ = g.generate(g.GEN_UNIFORM, 13159, 9_000_000)
+    refs = [reference.run(uxy, None, repeat=1, timeout=300) for _ in range(2)]
+    ours = g.Triangulator(max_points=len(uxy), max_segments=1, device=dev.index)
+    d_u = torch.from_numpy(uxy).to(dev)
+    ours_ms, (tris, _, _) = _time_solves(ours, d_u, None, max(5, args.steps // 2), 3, dev)
+    ours_tris = tris.cpu().numpy()
+    ours.close()
+    same = bool(np.array_equal(g.canonical(ours_tris), g.canonical(refs[-1]["tris"])))
+    ref_ms = statistics.median([x["event_ms"] for x in refs])
+    res["uniform_9m"] = {
+        "ref_ms": ref_ms, "ref_ms_runs": [x["event_ms"] for x in refs],
+        "ref_sum_time_ms": refs[-1]["sum_time"], "ref_final_mark": refs[-1]["marks"][-1] if refs[-1]["marks"] else None,
+        "ours_ms": ours_ms, "speedup": ref_ms / ours_ms, "identical_triangle_set": same,
+        "n_points": len(uxy), "ref_mpts_per_s": len(uxy) / (ref_ms * 1e-3) / 1e6,
+        "ours_mpts_per_s": len(uxy) / (ours_ms * 1e-3) / 1e6}
+    return res
+
+
+def measure_lattice(args, dev):
+    """The degenerate workload: a 2048 x 2048 lattice, spacing 2^14, 20,000
+    unit constraint segments (every empty circle through four neighbours is
+    a tie); device-resident solves, the output checked by the exact
+    validator."""
+    import torch
+    import gcdt_b200 as g
+    from oracle import oracle
+    xy, cons = g.generate(g.GEN_LATTICE, 1)
+    tri = g.Triangulator(max_points=len(xy), max_segments=len(cons), device=dev.index)
+    ms, (tris, adj, cf) = _time_solves(tri, torch.from_numpy(xy).to(dev), torch.from_numpy(cons).to(dev),
+                                       args.steps, args.warmup, dev)
+    tri.close()
+    ok, msg = oracle.validate(xy, cons, tris.cpu().numpy(), adj.cpu().numpy(), cf.cpu().numpy())
+    return {"workload": "2048x2048 lattice, spacing 2^14, 20,000 unit segments", "n_points": len(xy),
+            "n_segments": len(cons), "n_triangles": int(tris.shape[0]), "ms": ms,
+            "mpts_per_s": len(xy) / (ms * 1e-3) / 1e6, "validated": ok if ok else msg}
 
 
 def apply_tuning(tri, args):
@@ -446,15 +573,21 @@ def apply_tuning(tri, args):
 
 
 def run_batched(args):
+    import torch
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    print(json.dumps(measure_batched(args, torch.device("cuda", local), args.steps, args.warmup,
+                                     args.validate, rank=rank)), flush=True)
+
+
+def measure_batched(args, dev, steps, warmup, validate, rank=0):
     """Batched workload: 4,096 independent instances, point counts log-uniform
     in [64, 65,536], coordinates in [1, 2^24), 1-4 star polygons of 16-256
     vertices each.  Reports instances/s of one batched call next to looping the
     plain solver over the same instances."""
     import torch
     import gcdt_b200 as g
-    rank, world, local = rank_info()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
+    local = dev.index
     ninst = args.instances
     inst = [g.generate(g.GEN_BATCH_INSTANCE, 1 + rank * ninst + i) for i in range(ninst)]
     po, so = g.BatchTriangulator.offsets(inst)
@@ -466,11 +599,11 @@ def run_batched(args):
     cfg = bt.autotune(d_xy, d_c, po, so, sample_instances=min(256, ninst))
     out = bt.alloc_outputs(po)
     stream = torch.cuda.current_stream(dev)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         bt.triangulate_device(d_xy, d_c, po, so, out=out)
     torch.cuda.synchronize()
     ms = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         _, st, rc = bt.triangulate_device(d_xy, d_c, po, so, out=out)
         if rc != 0:
             raise RuntimeError("batched solve failed: %s" % g.STATUS.get(rc, rc))
@@ -481,7 +614,7 @@ def run_batched(args):
     h_c = torch.from_numpy(cons).pin_memory()
     h_out = tuple(torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in out)
     e2e = []
-    for k in range(args.warmup + args.steps):
+    for k in range(warmup + steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         d_xy.copy_(h_xy, non_blocking=True)
@@ -491,7 +624,7 @@ def run_batched(args):
             hd.copy_(dd, non_blocking=True)
         b.record(stream)
         b.synchronize()
-        if k >= args.warmup:
+        if k >= warmup:
             e2e.append(a.elapsed_time(b))
     e2e_ms = statistics.median(e2e)
     # looping the plain solver over the same device-resident instances
@@ -509,7 +642,7 @@ def run_batched(args):
     loop_ms = a.elapsed_time(b)
     # equality with the plain solver on a sample of instances
     same = True
-    if args.validate:
+    if validate:
         tris_h, adj_h, cf_h = (o.cpu().numpy() for o in out)
         for i in range(0, ninst, max(1, ninst // 64)):
             t0 = int(2 * po[i] + 2 * i); t1 = t0 + 2 * len(inst[i][0]) + 2
@@ -518,7 +651,7 @@ def run_batched(args):
     tri.close()
     line = {
         "metric": "batched vs looped inst/s", "value": ninst / (batch_ms * 1e-3), "unit": "instances/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms,
+        "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": batch_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "i64/i128 exact predicates on i32 coordinates (f64 filter)", "data": "synthetic",
         "config": {"workload": "batched: %d instances, n log-uniform [64, 65536], coords [1, 2^24), 1-4 star polygons of 16-256 vertices" % ninst,
@@ -529,10 +662,10 @@ def run_batched(args):
         "e2e": {"value": ninst / (e2e_ms * 1e-3), "unit": "instances/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(xy.nbytes + cons.nbytes),
                 "d2h_bytes_per_step": int(sum(o.numel() * o.element_size() for o in out))},
-        "equal_to_plain_solver_sample": same if args.validate else None,
+        "equal_to_plain_solver_sample": same if validate else None,
     }
-    print(json.dumps(line), flush=True)
     bt.close()
+    return line
 
 
 def run_export(args):
@@ -605,6 +738,10 @@ def run_export(args):
 
 
 def run_serving(args):
+    print(json.dumps(measure_serving(args)), flush=True)
+
+
+def measure_serving(args):
     """Serving stream: requests with point counts log-uniform in
     [1,000, 1,000,000] (the scale workload's Gaussian/uniform mix in
     [1, 2^28)^2, star polygons totalling ~2% of the points), Poisson
@@ -674,8 +811,8 @@ def run_serving(args):
                    "points_served": pts, "wall_s": wall},
         "server_stats": st,
     }
-    print(json.dumps(line), flush=True)
     sv.close()
+    return line
 
 
 def main():
@@ -693,9 +830,12 @@ def main():
     ap.add_argument("--pool", type=int, default=256)
     ap.add_argument("--big-points", type=int, default=8000,
                     help="serving: requests with at least this many points use the whole-GPU solve")
-    ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-repeat", type=int, default=3)
-    ap.add_argument("--validate", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the single-threaded CPU oracle leg")
+    ap.add_argument("--no-validate", action="store_true", help="skip the exact validation of the timed output")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the extra measurements (reference CUDA build, lattice, batched, serving)")
+    ap.add_argument("--validate", action="store_true",
+                    help="batched: compare a sample of instances with the plain solver")
     ap.add_argument("--scale-points", type=int, default=0,
                     help="profiling only: a reduced copy of the workload with this many generated points")
     ap.add_argument("--levels", type=int, default=None, help="insertion levels (1-4)")

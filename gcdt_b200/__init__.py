@@ -66,8 +66,8 @@ class Stats(ctypes.Structure):
 
 def lib_path():
     """The CUDA library: libgcdt_b200.so next to this file, or the build
-    variant named by GCDT_B200_LIB (a path, or a variant name such as
-    "oneside" for libgcdt_b200_oneside.so; see build.VARIANTS)."""
+    variant named by GCDT_B200_LIB (a path, or a variant name NAME for
+    libgcdt_b200_NAME.so next to this file; see build.VARIANTS)."""
     v = os.environ.get("GCDT_B200_LIB")
     if v:
         return v if os.sep in v else os.path.join(_HERE, "libgcdt_b200_%s.so" % v)

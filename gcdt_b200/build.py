@@ -58,9 +58,8 @@ def _deps(*names):
 
 # Compile-time variants of the solver bodies, built next to the default
 # library for measurement (GCDT_B200_LIB selects one at import):
-#   oneside  GCDT_FLIP_ONE_SIDE: an edge of two triangles split in the same
-#            round, or flipped in the same sub-round, is tested from one side.
-VARIANTS = {"oneside": ["-DGCDT_FLIP_ONE_SIDE"]}
+#   name -> extra nvcc flags.  None at present.
+VARIANTS = {}
 
 
 def build(force=False, verbose=False, ptxas_verbose=False, variant=None):

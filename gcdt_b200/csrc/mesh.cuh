@@ -615,26 +615,6 @@ GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
     }
 }
 
-#ifdef GCDT_FLIP_ONE_SIDE
-// resolve_split_edge, returning (1 << s) when the triangle across the old
-// edge was split this round too and its child there has the smaller id: that
-// child's queue entry tests the edge, so this one need not.
-GCDT_HD int resolve_split_edge_dup(const Ctx& c, int ch, int s) {
-    int4* row = &tri_a(c, ch);
-    int old = comp(*row, s);
-    if (old < 0) return 0;
-    int m = old >> 2, ms = old & 3;
-    int2 im = c.ins[m];
-    if (im.x == (int)c.round) {
-        int other = split_child(im, m, ms);
-        ((int*)row)[s] = enc(other, ms);
-        return other < ch ? (1 << s) : 0;
-    }
-    ((int*)&tri_a(c, m))[ms] = enc(ch, s);
-    return 0;
-}
-#endif
-
 // Resolve outer adjacency of the children of one inserted point and queue
 // them for the flip phase (c.sr = first sub-round of this round).
 GCDT_HD void body_fix(const Ctx& c, int k) {
@@ -647,35 +627,17 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
     // so the circle through q and the spoke's far edge excludes the third
     // corner; on an edge split the spoke's quadrilateral is not even convex).
     if (code == 7) {
-#ifdef GCDT_FLIP_ONE_SIDE
-        int m0 = resolve_split_edge_dup(c, t, 0), m1 = resolve_split_edge_dup(c, T1, 1);
-        int m2 = resolve_split_edge_dup(c, T2, 2);
-        // children whose only old edge the other side tests are not queued
-        const int keep = !m0 + !m1 + !m2;
-        int* qn = c.queue_next + append_slots(&c.cnt->cur_q, c.base_q, keep);
-        if (!m0) *qn++ = qentry(t, 1);
-        if (!m1) *qn++ = qentry(T1, 2);
-        if (!m2) *qn++ = qentry(T2, 4);
-#else
         resolve_split_edge(c, t, 0);
         resolve_split_edge(c, T1, 1);
         resolve_split_edge(c, T2, 2);
         int* qn = c.queue_next + append_slots(&c.cnt->cur_q, c.base_q, 3);
         qn[0] = qentry(t, 1); qn[1] = qentry(T1, 2); qn[2] = qentry(T2, 4);
-#endif
     } else {
         int e = code;
         int e1 = nx3(e), e_2 = nx3(e1);
         int en = comp(tri_a(c, T1), e);     // A2 slot e = enc(B1, e2)
         int n = en >> 2, e2 = en & 3;
         int f1 = nx3(e2), f2 = nx3(f1);
-#ifdef GCDT_FLIP_ONE_SIDE
-        int m0 = resolve_split_edge_dup(c, t, e1), m1 = resolve_split_edge_dup(c, T1, e_2);
-        int m2 = resolve_split_edge_dup(c, n, f1), m3 = resolve_split_edge_dup(c, T2, f2);
-        int* qn = c.queue_next + append_slots(&c.cnt->cur_q, c.base_q, 4);
-        qn[0] = qentry(t, ((1 << e1) & ~m0) | (1 << e)); qn[1] = qentry(T1, ((1 << e_2) & ~m1) | (1 << e));
-        qn[2] = qentry(n, ((1 << f1) & ~m2) | (1 << e2)); qn[3] = qentry(T2, ((1 << f2) & ~m3) | (1 << e2));
-#else
         resolve_split_edge(c, t, e1);
         resolve_split_edge(c, T1, e_2);
         resolve_split_edge(c, n, f1);
@@ -684,7 +646,6 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
         int* qn = c.queue_next + append_slots(&c.cnt->cur_q, c.base_q, 4);
         qn[0] = qentry(t, (1 << e1) | (1 << e)); qn[1] = qentry(T1, (1 << e_2) | (1 << e));
         qn[2] = qentry(n, (1 << f1) | (1 << e2)); qn[3] = qentry(T2, (1 << f2) | (1 << e2));
-#endif
     }
 }
 
@@ -701,9 +662,6 @@ GCDT_HD void body_flip_check(const Ctx& c, int k) {
     // a carried entry whose triangle was split this round: the split's own
     // queue entries test every old edge of it
     if (k < c.carry_n && c.ins[t].x == (int)c.round) { c.cand[k] = make_int2(-1, -1); return; }
-#ifdef GCDT_FLIP_ONE_SIDE
-    if (mask == 0) { c.cand[k] = make_int2(-1, -1); return; }
-#endif
     int4 tv = tri_v(c, t), ta = tri_a(c, t);
     // the edges to test: in the mask, with a neighbour, not constraints
     int live = mask & ~tv.w & ((ta.x >= 0) | ((ta.y >= 0) << 1) | ((ta.z >= 0) << 2));
@@ -748,11 +706,6 @@ GCDT_HD void flip_check_multi(const Ctx& c, const int (&ks)[W]) {
 #pragma unroll
     for (int u = 0; u < W; ++u)
         if (on[u] && ks[u] < c.carry_n && c.ins[t[u]].x == (int)c.round) on[u] = false;
-#ifdef GCDT_FLIP_ONE_SIDE
-#pragma unroll
-    for (int u = 0; u < W; ++u)
-        if (mask[u] == 0) on[u] = false;
-#endif
     int4 tv[W], ta[W];
 #pragma unroll
     for (int u = 0; u < W; ++u) {
@@ -881,30 +834,6 @@ GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
     }
 }
 
-#ifdef GCDT_FLIP_ONE_SIDE
-// One-sided edge tests (compiled only where GCDT_FLIP_ONE_SIDE is defined):
-// an outer edge whose neighbour was flipped in the same sub-round is in both
-// new triangles' queue masks; only the triangle with the smaller id keeps
-// it.  The neighbour's own fix makes the mirror decision, so exactly one
-// side tests the edge next sub-round.  Returns the bit to clear.
-GCDT_HD int one_side_bit(int tt, int s, int new_nb) { return (new_nb >> 2) < tt ? (1 << s) : 0; }
-
-GCDT_HD int resolve_flip_edge_dup(const Ctx& c, int tt, int s) {
-    int4* row = &tri_a(c, tt);
-    int old = comp(*row, s);
-    if (old < 0) return 0;
-    int m = old >> 2, ms = old & 3;
-    int4 fm = c.fmap[m];
-    if (fm.w == (int)c.sr) {
-        int nw = comp(fm, ms);
-        ((int*)row)[s] = nw;
-        return one_side_bit(tt, s, nw);
-    }
-    ((int*)&tri_a(c, m))[ms] = enc(tt, s);
-    return 0;
-}
-#endif
-
 // k < c.list_n: resolve the outer adjacency of flipped pair k.
 // Otherwise queue entry k - c.list_n: a candidate that did not flip and
 // whose triangle nobody flipped goes back to the queue, after the
@@ -918,17 +847,10 @@ GCDT_HD void body_flip_fix(const Ctx& c, int k) {
     }
     int t = qtri(c.queue_next[2 * k]);
     int n = tri_a(c, t).y >> 2;
-#ifdef GCDT_FLIP_ONE_SIDE
-    int ct = resolve_flip_edge_dup(c, t, 0) | resolve_flip_edge_dup(c, t, 2);
-    int cn = resolve_flip_edge_dup(c, n, 0) | resolve_flip_edge_dup(c, n, 1);
-    if (ct) c.queue_next[2 * k] = qentry(t, 5 & ~ct);
-    if (cn) c.queue_next[2 * k + 1] = qentry(n, 3 & ~cn);
-#else
     resolve_flip_edge(c, t, 0);
     resolve_flip_edge(c, t, 2);
     resolve_flip_edge(c, n, 0);
     resolve_flip_edge(c, n, 1);
-#endif
 }
 
 // The edge in slot s of flipped triangle tt named the old neighbour `old`
@@ -992,15 +914,6 @@ GCDT_HD void body_flip_fix_pair(const Ctx& c, int k0, int k1) {
         resolve_flip_loaded(c, t[u], 2, ta[u].z, f2[u]);
         resolve_flip_loaded(c, n[u], 0, na[u].x, g0[u]);
         resolve_flip_loaded(c, n[u], 1, na[u].y, g1[u]);
-#ifdef GCDT_FLIP_ONE_SIDE
-        const int sr = (int)c.sr;
-        int ct = (ta[u].x >= 0 && f0[u].w == sr ? one_side_bit(t[u], 0, comp(f0[u], ta[u].x & 3)) : 0) |
-                 (ta[u].z >= 0 && f2[u].w == sr ? one_side_bit(t[u], 2, comp(f2[u], ta[u].z & 3)) : 0);
-        int cn = (na[u].x >= 0 && g0[u].w == sr ? one_side_bit(n[u], 0, comp(g0[u], na[u].x & 3)) : 0) |
-                 (na[u].y >= 0 && g1[u].w == sr ? one_side_bit(n[u], 1, comp(g1[u], na[u].y & 3)) : 0);
-        if (ct) c.queue_next[2 * ks[u]] = qentry(t[u], 5 & ~ct);
-        if (cn) c.queue_next[2 * ks[u] + 1] = qentry(n[u], 3 & ~cn);
-#endif
     }
 }
 

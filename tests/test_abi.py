@@ -96,8 +96,8 @@ def test_variant_library_selection(monkeypatch):
     import importlib
     monkeypatch.delenv("GCDT_B200_LIB", raising=False)
     assert g.lib_path().endswith(os.path.join("gcdt_b200", "libgcdt_b200.so"))
-    monkeypatch.setenv("GCDT_B200_LIB", "oneside")
-    assert g.lib_path().endswith(os.path.join("gcdt_b200", "libgcdt_b200_oneside.so"))
+    monkeypatch.setenv("GCDT_B200_LIB", "probe")
+    assert g.lib_path().endswith(os.path.join("gcdt_b200", "libgcdt_b200_probe.so"))
     monkeypatch.setenv("GCDT_B200_LIB", "/nonexistent/libx.so")
     assert g.lib_path() == "/nonexistent/libx.so"
     saved = g._LIB

@@ -154,56 +154,3 @@ def test_record_accesses_per_point():
     assert fo["flips"] <= fo["distinct_candidates"] <= fo["with_candidate"] <= fo["entries"]
     flips = acc.get("flip_check", 0) + acc.get("flip_do", 0) + acc.get("flip_fix", 0)
     assert 0.5 < flips / total < 0.75
-
-
-ONE_SIDE = ("GCDT_FLIP_ONE_SIDE",)
-
-
-@pytest.mark.parametrize("order", [0, 1, 2], ids=["forward", "reversed", "shuffled"])
-def test_one_sided_edge_tests_give_the_oracle_cdt(order):
-    """The one-sided variant of the fix bodies (built only here, with
-    GCDT_FLIP_ONE_SIDE): a shared edge of two triangles split in the same
-    round, or flipped in the same sub-round, stays in one queue mask only.
-    The result must still be the oracle's CDT, the same bytes in every item
-    order and with the one-item and paired bodies."""
-    L = ctypes.CDLL(build_host_emulation(ONE_SIDE))
-    vp, i32 = ctypes.c_void_p, ctypes.c_int
-    L.host_triangulate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, i32, i32, i32]
-    L.host_triangulate.restype = i32
-    for xy, cons in [g.generate(g.GEN_SMALL, 3), g.generate(g.GEN_LATTICE, 2, 128, 1000),
-                     g.generate(g.GEN_SCALE, 2, 100000, 6, 30)]:
-        n, s, T = len(xy), len(cons), 2 * len(xy) + 2
-        xy = np.ascontiguousarray(xy, np.int32)
-        cons = np.ascontiguousarray(cons, np.int32).reshape(-1, 2)
-        outs = []
-        for width in (1, 2):
-            out = [np.zeros((T, 3), np.int32), np.zeros((T, 3), np.int32), np.zeros(T, np.uint8)]
-            st = np.zeros(8, np.int64)
-            p = lambda a: ctypes.c_void_p(a.ctypes.data)
-            rc = L.host_triangulate(p(xy), n, p(cons), s, p(out[0]), p(out[1]), p(out[2]), p(st), order, width, 1)
-            assert rc == 0
-            outs.append(out)
-        assert all(np.array_equal(a, b) for a, b in zip(*outs))
-        ok, msg = oracle.validate(xy, cons, *outs[0])
-        assert ok, msg
-        orc, otris, _, _, _ = oracle.cdt(xy, cons)
-        assert orc == 0 and np.array_equal(g.canonical(outs[0][0]), g.canonical(otris))
-
-
-def test_one_sided_edge_tests_cut_duplicate_candidates():
-    """Access model of the one-sided variant at 200k points: the same flips,
-    about 70% fewer duplicate candidates and about 17% fewer flip-check
-    record accesses than the default bodies."""
-    n, a0, _ = record_accesses(200000)
-    f0 = dict(record_accesses.flip_outcomes)
-    n, a1, _ = record_accesses(200000, defines=ONE_SIDE)
-    f1 = dict(record_accesses.flip_outcomes)
-    print("flip_check %.2f -> %.2f accesses/point; candidates %.2f -> %.2f; total %.1f -> %.1f" % (
-        a0["flip_check"], a1["flip_check"], f0["with_candidate"], f1["with_candidate"],
-        sum(a0.values()), sum(a1.values())))
-    assert abs(f1["flips"] - f0["flips"]) < 0.05 * f0["flips"]
-    dup0 = f0["with_candidate"] - f0["distinct_candidates"]
-    dup1 = f1["with_candidate"] - f1["distinct_candidates"]
-    assert dup1 < 0.4 * dup0
-    assert a1["flip_check"] < 0.9 * a0["flip_check"]
-    assert f1["entries"] < 0.95 * f0["entries"]

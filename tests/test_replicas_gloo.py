@@ -67,12 +67,15 @@ def test_replica_workloads_are_seeded_per_rank():
     assert not np.array_equal(a0[:1000], a1[:1000])
 
 
-def test_reference_arm_runs_one_sample_per_thread():
-    """The --impl reference leg: every thread solves its own seeded sample,
-    all of them complete, and the step figure is all points over the step."""
+def test_reference_arm_runs_one_instance_per_thread():
+    """The --impl reference leg: every thread solves its own seeded instance
+    (reduced here), all of them complete, thread 0's is the headline
+    instance, and the step figure is all points over the step."""
     import bench
-    runs, desc = bench.cpu_oracle_parallel(2, 2, points=30000)
-    assert len(runs) == 2 and desc.startswith("2 concurrent samples")
+    runs, desc, (n0, s0) = bench.cpu_oracle_parallel(2, 2, scale_points=30000)
+    xy, cons = bench.replica_workload(0, scale_points=30000)
+    assert (n0, s0) == (len(xy), len(cons))
+    assert len(runs) == 2 and desc.startswith("2 concurrent reduced")
     total = int(desc.split(" points in all")[0].rsplit(" ", 1)[1])
     for v, t in runs:
         assert t > 0 and abs(v - total / t / 1e6) < 1e-9
