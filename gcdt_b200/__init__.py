@@ -92,6 +92,8 @@ def lib():
     L.gcdt_workspace_bytes.restype = ctypes.c_size_t
     L.gcdt_triangulate.argtypes = [vp, vp, i32, vp, i32, vp, vp, vp, ctypes.POINTER(i32), vp]
     L.gcdt_triangulate.restype = ctypes.c_int
+    L.gcdt_set_grid_blocks.argtypes = [vp, i32]
+    L.gcdt_set_grid_blocks.restype = ctypes.c_int
     L.gcdt_triangulate_async.argtypes = [vp, vp, i32, vp, i32, vp, vp, vp, vp]
     L.gcdt_triangulate_async.restype = ctypes.c_int
     L.gcdt_wait.argtypes = [vp, ctypes.POINTER(i32)]
@@ -102,6 +104,8 @@ def lib():
     L.gcdt_status_string.restype = ctypes.c_char_p
     L.gcdt_get_phase_profile.argtypes = [vp, vp, vp, i32]
     L.gcdt_get_phase_profile.restype = i32
+    L.gcdt_get_phase_balance.argtypes = [vp, vp, vp, vp, i32]
+    L.gcdt_get_phase_balance.restype = i32
     L.gcdt_phase_name.argtypes = [i32]
     L.gcdt_phase_name.restype = ctypes.c_char_p
     L.gcdt_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, i64, i64, i64]
@@ -160,6 +164,8 @@ def lib():
     L.gcdt_autotune.restype = ctypes.c_int
     L.gcdt_set_limits.argtypes = [vp, i32, i32, i32]
     L.gcdt_set_limits.restype = ctypes.c_int
+    L.gcdt_time_barriers.argtypes = [ctypes.c_int, i32, ctypes.POINTER(ctypes.c_double)]
+    L.gcdt_time_barriers.restype = ctypes.c_int
     L.gcdt_probe_barrier.argtypes = [ctypes.c_int, i32, i32, ctypes.c_uint32, ctypes.POINTER(i32)]
     L.gcdt_probe_barrier.restype = ctypes.c_int
     L.gcdt_classify_regions_scratch_bytes.argtypes = [i32]
@@ -291,6 +297,12 @@ class Triangulator:
             raise GcdtError(rc, "gcdt_triangulate")
         return tris, adj, cflags
 
+    def set_grid_blocks(self, blocks):
+        """Blocks of the persistent launch (0: one per SM), gcdt_set_grid_blocks."""
+        rc = lib().gcdt_set_grid_blocks(self._h, int(blocks))
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_set_grid_blocks")
+
     def triangulate_async(self, points, segments=None, out=None, stream=None):
         """Enqueue a solve on `stream` (default: the current stream) and return
         the output tensors at once; wait() reports the solve's status.  The
@@ -397,6 +409,22 @@ class Triangulator:
                 out[lib().gcdt_phase_name(i).decode()] = (int(cyc[i]), int(cnt[i]))
         return out
 
+    def phase_balance(self):
+        """{phase name: (longest block's work cycles, mean block's work
+        cycles)} summed over the runs of each grid phase of the last solve;
+        against phase_profile's cycles (block 0's view, barrier included)
+        they split a phase into barrier wait, imbalance and work."""
+        wmax = np.zeros(32, np.int64)
+        wsum = np.zeros(32, np.int64)
+        blocks = ctypes.c_int64(0)
+        k = lib().gcdt_get_phase_balance(self._h, ctypes.c_void_p(wmax.ctypes.data),
+                                         ctypes.c_void_p(wsum.ctypes.data), ctypes.byref(blocks), 32)
+        out = {}
+        for i in range(max(k, 0)):
+            if wmax[i]:
+                out[lib().gcdt_phase_name(i).decode()] = (int(wmax[i]), float(wsum[i]) / max(1, blocks.value))
+        return out
+
     def stats(self):
         st = Stats()
         rc = lib().gcdt_get_stats(self._h, ctypes.byref(st))
@@ -452,6 +480,16 @@ def reference_layout(points, tris, adj=None, cflags=None, stream=None):
     if rc != 0:
         raise GcdtError(rc, "gcdt_reference_layout")
     return pts_out, labels, tris_out, adj_out, cf_out
+
+
+def time_barriers(device=0, rounds=4096):
+    """Microseconds per grid barrier of the persistent kernel's executor
+    (gcdt_time_barriers)."""
+    us = ctypes.c_double(0)
+    rc = lib().gcdt_time_barriers(int(device), int(rounds), ctypes.byref(us))
+    if rc != 0:
+        raise GcdtError(rc, "gcdt_time_barriers")
+    return us.value
 
 
 def probe_barrier(device=0, blocks=4, absent_block=0, spin_limit=1 << 16):
@@ -616,7 +654,8 @@ class ServerConfig(ctypes.Structure):
                 ("max_batch_instances", ctypes.c_int32), ("max_batch_points", ctypes.c_int64),
                 ("max_batch_segments", ctypes.c_int64), ("lane_workspace_bytes", ctypes.c_int64),
                 ("big_request_points", ctypes.c_int64), ("max_request_points", ctypes.c_int64),
-                ("max_request_segments", ctypes.c_int64)]
+                ("max_request_segments", ctypes.c_int64), ("big_workers", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class ServerStats(ctypes.Structure):
@@ -635,10 +674,10 @@ class Server:
 
     def __init__(self, memory_budget_bytes=150 << 30, lanes=4, max_batch_instances=512,
                  max_batch_points=4_000_000, max_batch_segments=200_000, big_request_points=400_000,
-                 max_request_points=1_100_000, max_request_segments=40_000, device=0):
+                 max_request_points=1_100_000, max_request_segments=40_000, big_workers=1, device=0):
         cfg = ServerConfig(int(memory_budget_bytes), int(lanes), int(max_batch_instances), int(max_batch_points),
                            int(max_batch_segments), 0, int(big_request_points), int(max_request_points),
-                           int(max_request_segments))
+                           int(max_request_segments), int(big_workers), 0)
         h = ctypes.c_void_p()
         rc = lib().gcdt_server_create(ctypes.byref(h), int(device), ctypes.byref(cfg))
         if rc != 0:

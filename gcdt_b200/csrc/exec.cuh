@@ -16,7 +16,14 @@ namespace gcdt {
 // grid-stride loops separated by a grid barrier, so the round structure
 // costs no kernel launches and no host round trips.
 
-constexpr int kPersistBlock = 512;   // one block per SM (128 registers per thread)
+#ifndef GCDT_PERSIST_BLOCK
+#define GCDT_PERSIST_BLOCK 512
+#endif
+#ifndef GCDT_PERSIST_MINB
+#define GCDT_PERSIST_MINB 1
+#endif
+constexpr int kPersistBlock = GCDT_PERSIST_BLOCK;   // 512: one block per SM (128 registers per thread)
+constexpr int kPersistMinBlocks = GCDT_PERSIST_MINB;
 
 struct GridExec {
     static constexpr bool kCanNarrow = true;
@@ -42,8 +49,16 @@ struct GridExec {
     // spin_limit polls (2^24, about a second, in a solve) the block records
     // ST_BARRIER and stops waiting, and once that bit is set no block waits
     // or works any more, so the kernel always ends.
-    __device__ void barrier() {
+    __device__ void barrier() { barrier_timed(-1, 0, 0); }
+    // The barrier ending a phase: with k >= 0, thread 0 first records the
+    // block's work time (cycles since t0) for the phase balance.
+    __device__ void barrier_timed(int k, long long t0, int slot) {
         __syncthreads();
+        if (threadIdx.x == 0 && k >= 0) {
+            unsigned long long w = (unsigned long long)(clock64() - t0);
+            atomicMax(&cnt->wcur_max[slot], w);
+            atomicAdd(&cnt->wcur_sum[slot], w);
+        }
         if (threadIdx.x == 0) {
             volatile unsigned* vgen = &cnt->bar_gen;
             volatile int* vst = &cnt->status;
@@ -71,7 +86,7 @@ struct GridExec {
     }
     __device__ void phase(int k, const Ctx& c, long long count) {
         const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
-        long long t0 = timer ? clock64() : 0;
+        long long t0 = threadIdx.x == 0 ? clock64() : 0;
         if (!(word(&cnt->status) & ST_BARRIER)) {
             long long stride = (long long)gridDim.x * blockDim.x;
             long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -89,10 +104,18 @@ struct GridExec {
                 for (; i < count; i += stride) dispatch(k, c, (int)i);
             }
         }
-        barrier();
+        const int slot = c.eslot & 1;
+        barrier_timed(k < kMaxPhaseKinds ? k : -1, t0, slot);
         if (timer && k < kMaxPhaseKinds) {   // phase time incl. the barrier, as block 0 sees it
             cnt->phase_cyc[k] += clock64() - t0;
             cnt->phase_cnt[k] += 1;
+            // every block added this run's work time before it arrived; no
+            // block writes this slot again before the next barrier, which
+            // block 0 passes only after clearing it
+            cnt->phase_wmax[k] += (long long)*(volatile unsigned long long*)&cnt->wcur_max[slot];
+            cnt->phase_wsum[k] += (long long)*(volatile unsigned long long*)&cnt->wcur_sum[slot];
+            cnt->wcur_max[slot] = 0;
+            cnt->wcur_sum[slot] = 0;
         }
     }
     // Values read after a barrier come from the block's snapshot.
@@ -108,6 +131,7 @@ struct GridExec {
     }
     __device__ void finish(const Ctx&, long long rounds, long long subrounds, long long crounds, int rc) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
+            cnt->grid_blocks = nblocks;
             cnt->rounds = rounds;
             cnt->flip_subrounds = subrounds;
             cnt->constraint_rounds = crounds;
@@ -143,16 +167,13 @@ static_assert(sizeof(Driver) <= sizeof(((Counters*)0)->handoff), "driver state f
 static_assert(sizeof(Driver) % 8 == 0, "driver state is whole 8-byte words");
 
 __device__ inline void store_handoff(Counters* cnt, const Driver& D, long long nq, int rc) {
-    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&D);
-    for (unsigned k = 0; k < sizeof(Driver) / 8; ++k) cnt->handoff[k] = src[k];
+    save_driver(cnt, D);
     cnt->handoff_nq = nq;
     cnt->handoff_rc = rc;
 }
 
 __device__ inline int load_handoff(Counters* cnt, Driver& D, long long& nq) {
-    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&D);
-    volatile unsigned long long* src = cnt->handoff;
-    for (unsigned k = 0; k < sizeof(Driver) / 8; ++k) dst[k] = src[k];
+    load_driver(cnt, D);
     nq = *(volatile long long*)&cnt->handoff_nq;
     return *(volatile int*)&cnt->handoff_rc;
 }

@@ -38,7 +38,7 @@ __global__ void gcdt_predicates(const int2* q, int n, int* out) {
 
 static_assert(offsetof(Counters, cur_scr) + 8 <= GridExec::kSnapWords * 8, "cursors are in the snapshot");
 
-__global__ void __launch_bounds__(kPersistBlock, 1) gcdt_stages(Ctx c) {
+__global__ void __launch_bounds__(kPersistBlock, kPersistMinBlocks) gcdt_stages(Ctx c) {
     __shared__ unsigned long long snap[GridExec::kSnapWords];
     GridExec ex{c.cnt, gridDim.x, snap};
     if (threadIdx.x == 0) ex.take_snapshot();
@@ -55,6 +55,15 @@ __global__ void gcdt_barrier_probe(Counters* cnt, unsigned absent, unsigned spin
     GridExec ex{cnt, gridDim.x, snap, spin_limit};
     if (blockIdx.x == absent) return;
     ex.barrier();
+}
+
+// Cost of the persistent kernel's grid barrier: every block of a grid
+// shaped like the stage kernel's passes `rounds` barriers with no work
+// between them.
+__global__ void __launch_bounds__(kPersistBlock, kPersistMinBlocks) gcdt_barrier_loop(Counters* cnt, int rounds) {
+    __shared__ unsigned long long snap[GridExec::kSnapWords];
+    GridExec ex{cnt, gridDim.x, snap, 1u << 22};
+    for (int r = 0; r < rounds; ++r) ex.barrier();
 }
 
 constexpr int ST_CUDA = 32;
@@ -89,6 +98,7 @@ struct DeviceBackend {
     void fill(void* p, int v, size_t bytes) { note(cudaMemsetAsync(p, v, bytes, st)); }
     // All rounds run in one cooperative launch sized to the co-resident
     // block count, so every block is resident and the grid barrier is safe.
+    int grid_limit = 0;   // at most this many blocks (0: no limit)
     void stages(const Ctx& c) {
         if (err != cudaSuccess) return;
         int dev = 0, sms = 0, per_sm = 0;
@@ -96,10 +106,39 @@ struct DeviceBackend {
         note(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         note(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gcdt_stages, kPersistBlock, 0));
         if (err != cudaSuccess || sms <= 0 || per_sm <= 0) { note(cudaErrorLaunchOutOfResources); return; }
+        int blocks = sms * per_sm;
+        if (grid_limit > 0 && grid_limit < blocks) blocks = grid_limit;
         Ctx cc = c;
+#ifdef GCDT_PIN_POINTS
+        // measurement variant: the sorted point array as a persisting L2 window
+        int max_win = 0, max_persist = 0;
+        note(cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, dev));
+        note(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
+        size_t win = 8 * ((size_t)c.n + 4);
+        if (win > (size_t)max_win) win = (size_t)max_win;
+        if (win > (size_t)max_persist) win = (size_t)max_persist;
+        note(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, win));
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(blocks);
+        lc.blockDim = dim3(kPersistBlock);
+        lc.stream = st;
+        cudaLaunchAttribute at[2];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        at[1].id = cudaLaunchAttributeAccessPolicyWindow;
+        at[1].val.accessPolicyWindow.base_ptr = c.P;
+        at[1].val.accessPolicyWindow.num_bytes = win;
+        at[1].val.accessPolicyWindow.hitRatio = 1.0f;
+        at[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        at[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        lc.attrs = at;
+        lc.numAttrs = 2;
+        note(cudaLaunchKernelEx(&lc, gcdt_stages, cc));
+#else
         void* args[] = {&cc};
-        note(cudaLaunchCooperativeKernel((const void*)gcdt_stages, dim3(sms * per_sm), dim3(kPersistBlock),
+        note(cudaLaunchCooperativeKernel((const void*)gcdt_stages, dim3(blocks), dim3(kPersistBlock),
                                          args, 0, st));
+#endif
         launches++;
     }
     void read(Counters* h) {
@@ -172,6 +211,8 @@ struct gcdt_context {
     int32_t lim_rounds = 0, lim_subrounds = 0, lim_crounds = 0;
     // scheduling (gcdt_set_tuning)
     gcdt_tuning tuning = default_tuning();
+    // blocks of the persistent launch (0: all co-resident blocks)
+    int32_t grid_blocks = 0;
 };
 
 namespace {
@@ -231,15 +272,10 @@ extern "C" void gcdt_destroy(gcdt_context* ctx) {
     delete ctx;
 }
 
-extern "C" gcdt_status gcdt_triangulate_async(gcdt_context* ctx, const int32_t* d_points, int32_t n,
-                                              const int32_t* d_segments, int32_t s,
-                                              int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
-                                              void* stream) {
-    if (!ctx || n < 0 || s < 0 || (n > 0 && !d_points) || (s > 0 && !d_segments) ||
-        !d_tris || !d_adj || !d_cflags)
-        return GCDT_BAD_INPUT;
-    if (n > ctx->max_n || s > ctx->max_s) return GCDT_OOM;
-    if (ctx->pending) gcdt_wait(ctx, nullptr);   // one solve in flight per context
+namespace {
+// Enqueue a solve of (points, segments) on ctx.
+gcdt_status enqueue(gcdt_context* ctx, const int32_t* d_points, int32_t n, const int32_t* d_segments, int32_t s,
+                    int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags, void* stream) {
     DeviceGuard g(ctx->device);
     Plan plan = make_plan(n, s, sort_temp_bytes(n));
     if (plan.L.total > ctx->arena_bytes) return GCDT_OOM;
@@ -266,6 +302,7 @@ extern "C" gcdt_status gcdt_triangulate_async(gcdt_context* ctx, const int32_t* 
     bk.hcnt = ctx->hcnt;
     bk.sort_tmp = ctx->arena + plan.o_sort_tmp;
     bk.sort_bytes = plan.sort_temp_bytes;
+    bk.grid_limit = ctx->grid_blocks;
     bk.note(cudaEventRecord(ctx->ev0, bk.st));
     enqueue_solve(bk, c);
     bk.note(cudaMemcpyAsync(ctx->hcnt, c.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, bk.st));
@@ -276,6 +313,19 @@ extern "C" gcdt_status gcdt_triangulate_async(gcdt_context* ctx, const int32_t* 
     ctx->pend_launches = bk.launches;
     ctx->pend_err = bk.err;
     return bk.err == cudaSuccess ? GCDT_OK : GCDT_CUDA_ERROR;
+}
+}  // namespace
+
+extern "C" gcdt_status gcdt_triangulate_async(gcdt_context* ctx, const int32_t* d_points, int32_t n,
+                                              const int32_t* d_segments, int32_t s,
+                                              int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
+                                              void* stream) {
+    if (!ctx || n < 0 || s < 0 || (n > 0 && !d_points) || (s > 0 && !d_segments) ||
+        !d_tris || !d_adj || !d_cflags)
+        return GCDT_BAD_INPUT;
+    if (n > ctx->max_n || s > ctx->max_s) return GCDT_OOM;
+    if (ctx->pending) gcdt_wait(ctx, nullptr);   // one solve in flight per context
+    return enqueue(ctx, d_points, n, d_segments, s, d_tris, d_adj, d_cflags, stream);
 }
 
 extern "C" gcdt_status gcdt_wait(gcdt_context* ctx, int32_t* n_tris) {
@@ -307,6 +357,13 @@ extern "C" gcdt_status gcdt_wait(gcdt_context* ctx, int32_t* n_tris) {
     gcdt_status rc = map_status(bits);
     if (rc == GCDT_OK && n_tris) *n_tris = 2 * n + 2;
     return rc;
+}
+
+extern "C" gcdt_status gcdt_set_grid_blocks(gcdt_context* ctx, int32_t blocks) {
+    if (!ctx || blocks < 0) return GCDT_BAD_INPUT;
+    if (ctx->pending) gcdt_wait(ctx, nullptr);
+    ctx->grid_blocks = blocks;
+    return GCDT_OK;
 }
 
 extern "C" gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_points, int32_t n,
@@ -435,6 +492,44 @@ extern "C" gcdt_status gcdt_get_tuning(const gcdt_context* ctx, gcdt_tuning* tun
     return GCDT_OK;
 }
 
+extern "C" gcdt_status gcdt_time_barriers(int device, int32_t rounds, double* us_per_barrier) {
+    if (!us_per_barrier || rounds < 1 || rounds > (1 << 20)) return GCDT_BAD_INPUT;
+    *us_per_barrier = 0;
+    DeviceGuard g(device);
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gcdt_stages, kPersistBlock, 0) != cudaSuccess ||
+        sms <= 0 || per_sm <= 0) {
+        cudaGetLastError();
+        return GCDT_CUDA_ERROR;
+    }
+    Counters* cnt = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaMalloc(&cnt, sizeof(Counters)) != cudaSuccess) { cudaGetLastError(); return GCDT_CUDA_ERROR; }
+    cudaError_t e = cudaMemset(cnt, 0, sizeof(Counters));
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    float ms = 0.f;
+    int status = 0;
+    if (e == cudaSuccess) {
+        int r = rounds;
+        void* args[] = {&cnt, &r};
+        cudaEventRecord(a, 0);
+        e = cudaLaunchCooperativeKernel((const void*)gcdt_barrier_loop, dim3(sms * per_sm), dim3(kPersistBlock), args, 0, 0);
+        cudaEventRecord(b, 0);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e == cudaSuccess) e = cudaMemcpy(&status, &cnt->status, sizeof(int), cudaMemcpyDeviceToHost);
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    cudaFree(cnt);
+    if (e != cudaSuccess) { cudaGetLastError(); return GCDT_CUDA_ERROR; }
+    if (status & ST_BARRIER) return GCDT_INTERNAL;
+    *us_per_barrier = 1e3 * ms / rounds;
+    return GCDT_OK;
+}
+
 extern "C" gcdt_status gcdt_probe_barrier(int device, int32_t blocks, int32_t absent_block, uint32_t spin_limit,
                                           int32_t* timed_out) {
     if (!timed_out || blocks < 1 || blocks > 1024 || spin_limit == 0) return GCDT_BAD_INPUT;
@@ -546,6 +641,19 @@ extern "C" int32_t gcdt_get_phase_profile(const gcdt_context* ctx, int64_t* cycl
     for (int32_t k = 0; k < n && k < max_kinds; ++k) {
         if (cycles) cycles[k] = ctx->hcnt->phase_cyc[k];
         if (counts) counts[k] = ctx->hcnt->phase_cnt[k];
+    }
+    return n;
+}
+
+extern "C" int32_t gcdt_get_phase_balance(const gcdt_context* ctx, int64_t* wmax, int64_t* wsum, int64_t* blocks,
+                                          int32_t max_kinds) {
+    if (!ctx || !ctx->hcnt || max_kinds < 0) return -1;
+    if (blocks) *blocks = ctx->hcnt->grid_blocks;
+    int32_t n = (int32_t)(sizeof(kPhaseNames) / sizeof(kPhaseNames[0]));
+    if (n > kMaxPhaseKinds) n = kMaxPhaseKinds;
+    for (int32_t k = 0; k < n && k < max_kinds; ++k) {
+        if (wmax) wmax[k] = ctx->hcnt->phase_wmax[k];
+        if (wsum) wsum[k] = ctx->hcnt->phase_wsum[k];
     }
     return n;
 }

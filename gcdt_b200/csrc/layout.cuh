@@ -61,13 +61,15 @@ __host__ __device__ inline Plan make_plan(int64_t n, int64_t s, size_t sort_temp
     p.o_qst = L.take(4 * T);
     p.o_qA = L.take(4 * T);
     p.o_qB = L.take(4 * T);
+    p.o_scratch = L.take(4 * p.scratch_cap);
+    p.o_vt = L.take(4 * (nn + 4));
+    p.o_lvl = L.take(nn);
+    // the segment arrays last: every other array has the same offset for
+    // any segment count
     p.o_seg = L.take(16 * ss);
     p.o_pendA = L.take(4 * ss);
     p.o_pendB = L.take(4 * ss);
     p.o_pinfo = L.take(16 * ss);
-    p.o_scratch = L.take(4 * p.scratch_cap);
-    p.o_vt = L.take(4 * (nn + 4));
-    p.o_lvl = L.take(nn);
     return p;
 }
 

@@ -68,13 +68,22 @@ struct Counters {
     unsigned int bar_count;      // grid barrier
     unsigned int bar_gen;
     long long rounds, flip_subrounds, constraint_rounds;
-    long long pad1[3];
+    long long grid_blocks;       // blocks of the persistent launch
+    long long pad1[2];
     long long phase_cyc[kMaxPhaseKinds];   // SM cycles per phase kind (block 0's view)
     long long phase_cnt[kMaxPhaseKinds];
     unsigned long long handoff[24];        // driver state handed back by a single-block tail
     long long handoff_nq;
     int handoff_rc;
     int pad2;
+    // Balance of the grid phases: per phase kind, the sum over its runs of
+    // the longest and of the summed per-block work time (SM cycles from the
+    // phase's start to the block's arrival at the barrier).  wcur_* collect
+    // one run, double-buffered by phase parity.
+    long long phase_wmax[kMaxPhaseKinds];
+    long long phase_wsum[kMaxPhaseKinds];
+    unsigned long long wcur_max[2];
+    unsigned long long wcur_sum[2];
 };
 
 struct Ctx {

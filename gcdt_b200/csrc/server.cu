@@ -13,11 +13,15 @@
 //     arena) is free, so requests that arrive while others run are launched
 //     next to them and their work overlaps on the device;
 //   - requests of at least big_request_points points go to a second queue
-//     served by a worker thread that runs them one at a time on the whole GPU
-//     through the single-solve path, on a high-priority stream, concurrently
-//     with the lanes (the block scheduler favours the high-priority grid, and
-//     the single solve's bounded grid barrier turns any wait for blocks held
-//     by a lane into an error instead of a hang);
+//     served by big_workers worker threads, each running one request at a
+//     time through the single-solve path on its own context and
+//     high-priority stream, concurrently with the lanes.  One worker uses
+//     the whole GPU; k workers each launch the persistent stage kernel on
+//     1/k of the SMs (gcdt_set_grid_blocks), so k requests' grids fit the
+//     device together and the per-phase latencies of several mid-size
+//     solves overlap.  The block scheduler favours the high-priority grids,
+//     lane blocks always finish, and the stage kernel's bounded grid barrier
+//     turns any wait for blocks held elsewhere into an error, not a hang;
 //   - results stay resident in the output pool until the client fetches
 //     (copies out) or releases them.
 // Latency is measured on the host from submission to the moment the
@@ -112,14 +116,22 @@ double now_ms(std::chrono::steady_clock::time_point t0) {
 
 }  // namespace
 
+// A worker for large requests: its own solve context, input buffers and
+// high-priority stream.
+struct BigWorker {
+    gcdt_context* ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    int32_t* pts = nullptr;
+    int32_t* segs = nullptr;
+    std::thread th;
+};
+
 struct gcdt_server {
     int device = 0;
     gcdt_server_config cfg{};
     std::vector<Lane> lanes;
-    gcdt_context* big = nullptr;
-    cudaStream_t big_stream = nullptr, fetch_stream = nullptr;
-    int32_t* big_pts = nullptr;
-    int32_t* big_segs = nullptr;
+    std::vector<BigWorker> bigs;
+    cudaStream_t fetch_stream = nullptr;
     int32_t* pool_tris = nullptr;
     int32_t* pool_adj = nullptr;
     uint8_t* pool_cf = nullptr;
@@ -131,7 +143,7 @@ struct gcdt_server {
     std::deque<int64_t> big_queue;   // large requests, for the big worker
     std::unordered_map<int64_t, Request> reqs;
     int64_t next_id = 1;
-    std::thread th, big_th;
+    std::thread th;
     std::condition_variable big_cv;
     bool stop = false;
     gcdt_status fatal = GCDT_OK;
@@ -142,9 +154,9 @@ struct gcdt_server {
     size_t fixed_bytes = 0;
 
     void run();
-    void run_big_worker();
+    void run_big_worker(BigWorker& W);
     bool dispatch_batch(std::unique_lock<std::mutex>& lk, Lane& L);
-    bool run_big(std::unique_lock<std::mutex>& lk, int64_t id);
+    bool run_big(std::unique_lock<std::mutex>& lk, BigWorker& W, int64_t id);
     void complete(Request& r, gcdt_status st) {
         r.state = DONE;
         r.status = st;
@@ -228,9 +240,9 @@ bool gcdt_server::dispatch_batch(std::unique_lock<std::mutex>& lk, Lane& L) {
     return true;
 }
 
-// A large request on the whole GPU.  Returns false when the output pool
-// has no room yet.
-bool gcdt_server::run_big(std::unique_lock<std::mutex>& lk, int64_t id) {
+// A large request on worker W.  Returns false when the output pool has no
+// room yet.
+bool gcdt_server::run_big(std::unique_lock<std::mutex>& lk, BigWorker& W, int64_t id) {
     Request& r = reqs[id];
     int64_t ntri = 2 * (int64_t)r.n + 2;
     int64_t off = alloc.alloc(ntri);
@@ -246,23 +258,23 @@ bool gcdt_server::run_big(std::unique_lock<std::mutex>& lk, int64_t id) {
     const int32_t* cons = r.cons.data();
     int32_t n = r.n, s = r.s;
     lk.unlock();
-    cudaMemcpyAsync(big_pts, xy, 8 * (size_t)n, cudaMemcpyHostToDevice, big_stream);
-    if (s) cudaMemcpyAsync(big_segs, cons, 8 * (size_t)s, cudaMemcpyHostToDevice, big_stream);
+    cudaMemcpyAsync(W.pts, xy, 8 * (size_t)n, cudaMemcpyHostToDevice, W.stream);
+    if (s) cudaMemcpyAsync(W.segs, cons, 8 * (size_t)s, cudaMemcpyHostToDevice, W.stream);
     int32_t nt = 0;
-    gcdt_status rc = gcdt_triangulate(big, big_pts, n, s ? big_segs : nullptr, s, pool_tris + 3 * off,
-                                      pool_adj + 3 * off, pool_cf + off, &nt, big_stream);
+    gcdt_status rc = gcdt_triangulate(W.ctx, W.pts, n, s ? W.segs : nullptr, s, pool_tris + 3 * off,
+                                      pool_adj + 3 * off, pool_cf + off, &nt, W.stream);
     lk.lock();
     complete(reqs[id], rc);
     done_cv.notify_all();
     return true;
 }
 
-void gcdt_server::run_big_worker() {
+void gcdt_server::run_big_worker(BigWorker& W) {
     DevGuard g(device);
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
         if (stop && big_queue.empty()) break;
-        if (big_queue.empty() || !run_big(lk, big_queue.front()))
+        if (big_queue.empty() || !run_big(lk, W, big_queue.front()))
             big_cv.wait_for(lk, std::chrono::microseconds(100));
     }
 }
@@ -301,7 +313,7 @@ extern "C" gcdt_status gcdt_server_create(gcdt_server** out, int device, const g
     const gcdt_server_config& c = *cfg;
     if (c.lanes < 1 || c.lanes > 16 || c.max_batch_instances < 1 || c.max_batch_points < 1 ||
         c.max_batch_segments < 0 || c.max_request_points < 1 || c.max_request_points > GCDT_MAX_POINTS ||
-        c.max_request_segments < 0 || c.memory_budget_bytes <= 0)
+        c.max_request_segments < 0 || c.memory_budget_bytes <= 0 || c.big_workers < 0 || c.big_workers > 16)
         return GCDT_BAD_INPUT;
     gcdt_server* sv = new (std::nothrow) gcdt_server();
     if (!sv) return GCDT_OOM;
@@ -325,14 +337,21 @@ extern "C" gcdt_status gcdt_server_create(gcdt_server** out, int device, const g
              cudaMalloc(&L.d_segs, 8 * (size_t)std::max<int64_t>(c.max_batch_segments, 1)) == cudaSuccess;
         fixed += (size_t)sv->cfg.lane_workspace_bytes + 8 * (size_t)(c.max_batch_points + c.max_batch_segments);
     }
-    ok = ok && gcdt_create(&sv->big, device, c.max_request_points, c.max_request_segments) == GCDT_OK &&
+    const int nbig = c.big_workers > 1 ? c.big_workers : 1;
+    int sms = 0;
+    ok = ok && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
          cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio) == cudaSuccess &&
-         cudaStreamCreateWithPriority(&sv->big_stream, cudaStreamNonBlocking, hi_prio) == cudaSuccess &&
-         cudaStreamCreateWithFlags(&sv->fetch_stream, cudaStreamNonBlocking) == cudaSuccess &&
-         cudaMalloc(&sv->big_pts, 8 * (size_t)c.max_request_points) == cudaSuccess &&
-         cudaMalloc(&sv->big_segs, 8 * (size_t)std::max<int64_t>(c.max_request_segments, 1)) == cudaSuccess;
-    fixed += gcdt_workspace_bytes(c.max_request_points, c.max_request_segments) +
-             8 * (size_t)(c.max_request_points + c.max_request_segments);
+         cudaStreamCreateWithFlags(&sv->fetch_stream, cudaStreamNonBlocking) == cudaSuccess;
+    sv->bigs = std::vector<BigWorker>(nbig);
+    for (BigWorker& W : sv->bigs) {
+        ok = ok && gcdt_create(&W.ctx, device, c.max_request_points, c.max_request_segments) == GCDT_OK &&
+             (nbig == 1 || gcdt_set_grid_blocks(W.ctx, std::max(1, sms / nbig)) == GCDT_OK) &&
+             cudaStreamCreateWithPriority(&W.stream, cudaStreamNonBlocking, hi_prio) == cudaSuccess &&
+             cudaMalloc(&W.pts, 8 * (size_t)c.max_request_points) == cudaSuccess &&
+             cudaMalloc(&W.segs, 8 * (size_t)std::max<int64_t>(c.max_request_segments, 1)) == cudaSuccess;
+        fixed += gcdt_workspace_bytes(c.max_request_points, c.max_request_segments) +
+                 8 * (size_t)(c.max_request_points + c.max_request_segments);
+    }
     sv->fixed_bytes = fixed;
     int64_t pool_bytes = c.memory_budget_bytes - (int64_t)fixed;
     int64_t cap = pool_bytes / kTriBytes;
@@ -351,25 +370,24 @@ extern "C" gcdt_status gcdt_server_create(gcdt_server** out, int device, const g
     }
     sv->t0 = std::chrono::steady_clock::now();
     sv->th = std::thread([sv] { sv->run(); });
-    sv->big_th = std::thread([sv] { sv->run_big_worker(); });
+    for (BigWorker& W : sv->bigs) W.th = std::thread([sv, &W] { sv->run_big_worker(W); });
     *out = sv;
     return GCDT_OK;
 }
 
 extern "C" void gcdt_server_destroy(gcdt_server* sv) {
     if (!sv) return;
-    if (sv->th.joinable() || sv->big_th.joinable()) {
-        {
-            std::lock_guard<std::mutex> lk(sv->mu);
-            sv->stop = true;
-            sv->queue.clear();
-            sv->big_queue.clear();
-        }
-        sv->cv.notify_all();
-        sv->big_cv.notify_all();
-        if (sv->th.joinable()) sv->th.join();
-        if (sv->big_th.joinable()) sv->big_th.join();
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+        sv->queue.clear();
+        sv->big_queue.clear();
     }
+    sv->cv.notify_all();
+    sv->big_cv.notify_all();
+    if (sv->th.joinable()) sv->th.join();
+    for (BigWorker& W : sv->bigs)
+        if (W.th.joinable()) W.th.join();
     DevGuard g(sv->device);
     for (Lane& L : sv->lanes) {
         if (L.stream) cudaStreamSynchronize(L.stream);
@@ -381,11 +399,13 @@ extern "C" void gcdt_server_destroy(gcdt_server* sv) {
         cudaFree(L.d_pts);
         cudaFree(L.d_segs);
     }
-    gcdt_destroy(sv->big);
-    if (sv->big_stream) cudaStreamDestroy(sv->big_stream);
+    for (BigWorker& W : sv->bigs) {
+        gcdt_destroy(W.ctx);
+        if (W.stream) cudaStreamDestroy(W.stream);
+        cudaFree(W.pts);
+        cudaFree(W.segs);
+    }
     if (sv->fetch_stream) cudaStreamDestroy(sv->fetch_stream);
-    cudaFree(sv->big_pts);
-    cudaFree(sv->big_segs);
     cudaFree(sv->pool_tris);
     cudaFree(sv->pool_adj);
     cudaFree(sv->pool_cf);

@@ -14,6 +14,7 @@
 //      (addConstraints.cu:1723-1835 + the delaunayNew flip loop with noFlips)
 //   3  output in input index order with adjacency and constraint flags
 #pragma once
+#include <cstring>
 #include "layout.cuh"
 #include "mesh.cuh"
 
@@ -165,6 +166,21 @@ struct Driver {
     int nphase;
     int errs;
 };
+
+// The driver state handed between the grid and a single-block tail through
+// the counters' hand-off area, copied word by word through memcpy, which
+// keeps the copy well defined whatever the field types.
+GCDT_HD void save_driver(Counters* cnt, const Driver& D) {
+    unsigned long long w[sizeof(Driver) / 8];
+    memcpy(w, &D, sizeof(Driver));
+    for (unsigned k = 0; k < sizeof(Driver) / 8; ++k) cnt->handoff[k] = w[k];
+}
+GCDT_HD void load_driver(Counters* cnt, Driver& D) {
+    unsigned long long w[sizeof(Driver) / 8];
+    const volatile unsigned long long* src = cnt->handoff;
+    for (unsigned k = 0; k < sizeof(Driver) / 8; ++k) w[k] = src[k];
+    memcpy(&D, w, sizeof(Driver));
+}
 
 template <class EX>
 GCDT_HD void run_phase(EX& ex, Ctx& c, Driver& D, int k, long long count) {

@@ -2,10 +2,25 @@
 // on top of the B200 solver.  getSamplePoints, filterTriangles and getBitmap
 // are kernels of their own; the meshing stages establish their postcondition
 // with gcdt_triangulate on a context kept here and grown on demand.
+//
+// The reference's driver sequence (kernel.cu:5395-5448) asks for the same
+// triangulation more than once: delaunaySample re-triangulates the mesh
+// rawMeshBefore just built, and delaunayNew the one addConstraints just
+// built.  The surface keeps the last solve's output together with a
+// fingerprint of its inputs (a position-sensitive 64-bit hash of the points
+// and of the segments, computed on the device), and a stage whose inputs
+// match copies that output instead of solving again.  addConstraints solves
+// from the points with the segments.  Recovering them in rawMeshAfter's
+// finished mesh instead was measured 4.7x (1M points) and 2.2x (10M)
+// slower than that solve: at full density a segment crosses many triangles
+// and its flips run one after another, while the solve recovers segments
+// on its coarse first level.
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <climits>
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -19,13 +34,90 @@ constexpr int kLogSample = 8;          // 256 x 256 sample cells, math_base.cuh:
 constexpr int kLogBitmap = 10;         // 1024 x 1024 bitmap cells, math_base.cuh:25
 constexpr int kBoxR = (1 << kLogRes) - 1;
 
-std::mutex g_mu;
-gcdt_context* g_ctx = nullptr;
-int64_t g_n = -1, g_s = -1;
-int g_dev = -1;
-int32_t* g_adj = nullptr;
-uint8_t* g_cf = nullptr;
-int64_t g_tcap = 0;
+// A device buffer that only grows.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t bytes) {
+        if (bytes <= cap) return true;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 4 + 256;
+        if (cudaMalloc(&p, want) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cap = want;
+        return true;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// Buffers handed to the caller come from a stream-ordered memory pool of the
+// surface's own that keeps freed memory for reuse, so a stage that returns
+// new buffers on every call (as the reference's stages do from its MemCache)
+// does not pay for mapping fresh device memory each time.  The caller frees
+// them with cudaFree, which accepts pool allocations.  Where the pool cannot
+// be created, cudaMalloc.
+struct OutPool {
+    int dev = -1;
+    cudaMemPool_t pool = nullptr;
+    bool tried = false;
+    void bind(int device) {
+        if (tried && dev == device) return;
+        tried = true;
+        dev = device;
+        pool = nullptr;
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            pool = nullptr;
+            return;
+        }
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    template <class T>
+    bool alloc(T** p, size_t bytes) {
+        *p = nullptr;
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, pool, 0)
+                             : cudaMalloc(reinterpret_cast<void**>(p), bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            return false;
+        }
+        return true;
+    }
+};
+OutPool g_out;
+
+// State of the surface functions: one solver context, pooled scratch and the
+// last solve's output, all on one device (they move when the caller's
+// current device changes).  The reference's stage functions are called from
+// one host thread; the mutex keeps concurrent callers from interleaving.
+struct Surface {
+    std::mutex mu;
+    int dev = -1;
+    gcdt_context* ctx = nullptr;
+    int64_t ctx_n = -1, ctx_s = -1;
+    DevBuf scratch;                  // per-call scratch (never returned to the caller)
+    DevBuf scratch2;                 // fingerprint words, then CUB temporary storage
+    DevBuf pairs, keys;              // getBitmap's pair flags/positions and sort keys
+    DevBuf c_tris, c_adj, c_cf;      // last solve's output, input index order
+    bool have = false;
+    int64_t n = -1, s = -1;
+    unsigned long long hp = 0, hc = 0;
+};
+Surface g_sf;
 
 struct EventTimer {
     cudaEvent_t a = nullptr, b = nullptr;
@@ -45,6 +137,30 @@ struct EventTimer {
     }
 };
 
+// Switch the surface to the current device, dropping what lives on another.
+void bind_device() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev == g_sf.dev) return;
+    if (g_sf.dev >= 0) {
+        cudaSetDevice(g_sf.dev);
+        if (g_sf.ctx) gcdt_destroy(g_sf.ctx);
+        g_sf.scratch.release();
+        g_sf.scratch2.release();
+        g_sf.pairs.release();
+        g_sf.keys.release();
+        g_sf.c_tris.release();
+        g_sf.c_adj.release();
+        g_sf.c_cf.release();
+        cudaSetDevice(dev);
+    }
+    g_sf.ctx = nullptr;
+    g_sf.ctx_n = g_sf.ctx_s = -1;
+    g_sf.have = false;
+    g_sf.dev = dev;
+    g_out.bind(dev);
+}
+
 __global__ void write_corners(int2* p, int n) {
     int k = threadIdx.x;
     if (k < 4) p[n + k] = make_int2((k == 1 || k == 2) ? kBoxR : 0, k >= 2 ? kBoxR : 0);
@@ -55,69 +171,122 @@ __global__ void fill_ints(int* p, int v, int n) {
     if (i < n) p[i] = v;
 }
 
-// Triangulate points[0..n) (+ cons) into tris (+ adj); writes the box
-// corners at points[n..n+3].  Returns the triangle count or -1.
-int solve(Point2d* points, int n, const int2* cons, int s, int3* tris, int3* adj, const char* who) {
-    std::lock_guard<std::mutex> lk(g_mu);
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!g_ctx || dev != g_dev || n > g_n || s > g_s) {
-        if (g_ctx) gcdt_destroy(g_ctx);
-        g_ctx = nullptr;
-        int64_t nn = n > g_n ? n : g_n, ss = s > g_s ? s : g_s;
-        if (dev != g_dev) { nn = n; ss = s; }
-        if (gcdt_create(&g_ctx, dev, nn, ss) != GCDT_OK) {
-            fprintf(stderr, "%s: cannot create a context for %d points\n", who, n);
-            g_n = g_s = -1;
-            return -1;
-        }
-        g_n = nn;
-        g_s = ss;
-        g_dev = dev;
+// ---- input fingerprint: sum over i of mix(i, v[i]) (MurmurHash3's 64-bit
+// finalizer as the mixer), so any change of a value or of its position
+// changes the sum with overwhelming probability
+__device__ __forceinline__ unsigned long long fmix64(unsigned long long x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+__global__ void hash_pairs(const int2* v, int n, unsigned long long salt, unsigned long long* out) {
+    unsigned long long h = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int2 p = v[i];
+        unsigned long long w = ((unsigned long long)(unsigned)p.x << 32) | (unsigned)p.y;
+        h += fmix64(w ^ fmix64((unsigned long long)i * 0x9e3779b97f4a7c15ull + salt));
     }
-    int64_t T = 2 * (int64_t)n + 2;
-    if (T > g_tcap || dev != g_dev) {
-        cudaFree(g_adj);
-        cudaFree(g_cf);
-        g_adj = nullptr;
-        g_cf = nullptr;
-        if (cudaMalloc(&g_adj, 12 * T) != cudaSuccess || cudaMalloc(&g_cf, T) != cudaSuccess) {
-            cudaGetLastError();
-            g_tcap = 0;
-            fprintf(stderr, "%s: out of device memory\n", who);
-            return -1;
-        }
-        g_tcap = T;
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, h);
+}
+
+// Fingerprints of points[0..n) and cons[0..s) (one host read).
+bool fingerprint(const Point2d* points, int n, const int2* cons, int s, unsigned long long* hp,
+                 unsigned long long* hc) {
+    if (!g_sf.scratch2.ensure(256)) return false;
+    unsigned long long* d = static_cast<unsigned long long*>(g_sf.scratch2.p);
+    cudaMemsetAsync(d, 0, 16, 0);
+    if (n > 0) hash_pairs<<<592, 256>>>(points, n, 0x1234567ull, d);
+    if (s > 0 && cons) hash_pairs<<<148, 256>>>(cons, s, 0x89abcdefull, d + 1);
+    unsigned long long h[2] = {0, 0};
+    if (cudaMemcpy(h, d, 16, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    *hp = h[0];
+    *hc = h[1];
+    return true;
+}
+
+// The constrained Delaunay triangulation of points[0..n) (+ cons) into the
+// cache (c_tris, c_adj, c_cf): from the cache where the fingerprint
+// matches, else by a solve.  Writes the box corners at points[n..n+3].
+// Returns the triangle count or -1.
+int solve_cached(Point2d* points, int n, const int2* cons, int s, const char* who) {
+    bind_device();
+    if (s > 0 && !cons) {
+        fprintf(stderr, "%s: %d segments without a segment array\n", who, s);
+        return -1;
+    }
+    unsigned long long hp = 0, hc = 0;
+    if (!fingerprint(points, n, cons, s, &hp, &hc)) {
+        fprintf(stderr, "%s: device error\n", who);
+        return -1;
+    }
+    const int64_t T = 2 * (int64_t)n + 2;
+    if (g_sf.have && g_sf.n == n && g_sf.s == s && g_sf.hp == hp && g_sf.hc == hc) {
+        write_corners<<<1, 32>>>(points, n);
+        return (int)T;
+    }
+    if (!g_sf.c_tris.ensure(12 * T) || !g_sf.c_adj.ensure(12 * T) || !g_sf.c_cf.ensure(T)) {
+        fprintf(stderr, "%s: out of device memory\n", who);
+        g_sf.have = false;
+        return -1;
     }
     int32_t nt = 0;
-    gcdt_status rc = gcdt_triangulate(g_ctx, reinterpret_cast<const int32_t*>(points), n,
-                                      reinterpret_cast<const int32_t*>(cons), s, reinterpret_cast<int32_t*>(tris),
-                                      adj ? reinterpret_cast<int32_t*>(adj) : g_adj, g_cf, &nt, nullptr);
+    g_sf.have = false;
+    if (!g_sf.ctx || n > g_sf.ctx_n || s > g_sf.ctx_s) {
+        int64_t nn = n > g_sf.ctx_n ? n : g_sf.ctx_n, ss = s > g_sf.ctx_s ? s : g_sf.ctx_s;
+        if (g_sf.ctx) gcdt_destroy(g_sf.ctx);
+        g_sf.ctx = nullptr;
+        g_sf.ctx_n = g_sf.ctx_s = -1;
+        if (gcdt_create(&g_sf.ctx, g_sf.dev, nn, ss) != GCDT_OK) {
+            fprintf(stderr, "%s: cannot create a context for %d points\n", who, n);
+            return -1;
+        }
+        g_sf.ctx_n = nn;
+        g_sf.ctx_s = ss;
+    }
+    gcdt_status rc = gcdt_triangulate(g_sf.ctx, reinterpret_cast<const int32_t*>(points), n,
+                                      reinterpret_cast<const int32_t*>(cons), s, static_cast<int32_t*>(g_sf.c_tris.p),
+                                      static_cast<int32_t*>(g_sf.c_adj.p), static_cast<uint8_t*>(g_sf.c_cf.p), &nt, nullptr);
     if (rc != GCDT_OK) {
         fprintf(stderr, "%s: %s\n", who, gcdt_status_string(rc));
         return -1;
     }
+    g_sf.have = true;
+    g_sf.n = n;
+    g_sf.s = s;
+    g_sf.hp = hp;
+    g_sf.hc = hc;
     write_corners<<<1, 32>>>(points, n);
     return nt;
+}
+
+// Copy the cached triangulation out (tris and/or adj may be null).
+void copy_out(int3* tris, int3* adj, int nt) {
+    if (tris) cudaMemcpyAsync(tris, g_sf.c_tris.p, 12 * (size_t)nt, cudaMemcpyDeviceToDevice, 0);
+    if (adj) cudaMemcpyAsync(adj, g_sf.c_adj.p, 12 * (size_t)nt, cudaMemcpyDeviceToDevice, 0);
 }
 
 void mark_live(int* sons, int nt) {
     if (sons && nt > 0) fill_ints<<<(nt + 255) / 256, 256>>>(sons, -1, nt);
 }
 
-// exclusive sum with the caller's CUB scratch when it is large enough
+// Scratch for an exclusive sum of n ints: the caller's CUB scratch when it
+// is large enough, else the pooled buffer.
 bool exclusive_sum(void* cubTemp, size_t cubBytes, int* in, int* out, int n) {
     size_t need = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, need, in, out, n);
     void* tmp = cubTemp;
-    bool own = false;
     if (!cubTemp || cubBytes < need) {
-        if (cudaMalloc(&tmp, need > 0 ? need : 1) != cudaSuccess) { cudaGetLastError(); return false; }
-        own = true;
+        if (!g_sf.scratch2.ensure(need + 256)) return false;
+        tmp = static_cast<char*>(g_sf.scratch2.p) + 256;   // the first 256 bytes hold the fingerprint words
     }
-    cub::DeviceScan::ExclusiveSum(tmp, need, in, out, n);
-    if (own) cudaFree(tmp);
-    return true;
+    return cub::DeviceScan::ExclusiveSum(tmp, need, in, out, n) == cudaSuccess;
 }
 
 int read_int(const int* p) {
@@ -126,13 +295,17 @@ int read_int(const int* p) {
     return v;
 }
 
-// ---- getSamplePoints: the smallest index of each 2^22-wide cell
+// ---- getSamplePoints (rawMesh.cu:678-746): one point per 2^22-wide cell of
+// a 256 x 256 grid; cell (x, y) has the reference's number x * 256 + y
+// (rawMesh.cu:686), the samples come out in that order.  The reference keeps
+// whichever point of a cell wrote last; here the smallest input index, so
+// the result is deterministic and one of the reference's possible outputs.
 __global__ void sample_cells(const int2* pts, int n, int* cell_min) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int2 p = pts[i];
-    int shift = kLogRes - kLogSample;
-    int cell = (p.x >> shift) + ((p.y >> shift) << kLogSample);
+    const int shift = kLogRes - kLogSample;
+    int cell = ((p.x >> shift) << kLogSample) + (p.y >> shift);
     atomicMin(&cell_min[cell], i);
 }
 __global__ void sample_flags(const int* cell_min, int* flag, int ncell) {
@@ -167,94 +340,136 @@ __global__ void compact_tris(const int3* tris, int3* ntris, const int3* adj, int
     }
 }
 
-// ---- getBitmap: cells of a 1024 x 1024 grid met by each triangle, row by row
-__device__ bool row_span(int2 a, int2 b, int2 c, int row, int* c0, int* c1) {
-    const int shift = kLogRes - kLogBitmap;
-    double y0 = double((long long)row << shift), y1 = double(((long long)row + 1) << shift);
-    double lo = 1e30, hi = -1e30;
-    int2 v[3] = {a, b, c};
-    for (int k = 0; k < 3; ++k) {
-        int2 p = v[k], q = v[(k + 1) % 3];
-        if (p.y >= y0 && p.y <= y1) { lo = fmin(lo, double(p.x)); hi = fmax(hi, double(p.x)); }
-        for (int side = 0; side < 2; ++side) {
-            double yy = side ? y1 : y0;
-            if ((p.y - yy) * (q.y - yy) < 0.0) {
-                double x = p.x + (q.x - p.x) * (yy - p.y) / double(q.y - p.y);
-                lo = fmin(lo, x);
-                hi = fmax(hi, x);
-            }
-        }
-    }
-    if (lo > hi) return false;
-    const int cells = 1 << kLogBitmap;
-    int l = int(floor(lo - 1.0)) >> shift, h = int(ceil(hi + 1.0)) >> shift;   // one unit of slack
-    *c0 = max(0, l);
-    *c1 = min(cells - 1, h);
-    return *c0 <= *c1;
-}
-__device__ void tri_rows(const int2* pts, int3 t, int2* a, int2* b, int2* c, int* r0, int* r1) {
+// ---- getBitmap (boostmap.cu:146-181): for each cell (X, Y) of a 1024 x 1024
+// grid over the box -- the closed integer square [X a, X a + a - 1] x
+// [Y a, Y a + a - 1], a = 2^20, numbered X * 1024 + Y as in the reference --
+// the triangles whose closed area meets it, by exact integer tests, listed
+// in increasing triangle id.
+//
+// Cells of a triangle's bounding box, one thread per (triangle, cell) pair
+// after a scan of the per-triangle counts (the reference does the same,
+// countTriAABB + intersectSquareTri_s1, boostmap.cu:5-28, 67-113).
+__device__ __forceinline__ void tri_cells(const int2* pts, int3 t, int2* a, int2* b, int2* c, int* x0, int* y0,
+                                          int* nx, int* ny) {
     const int shift = kLogRes - kLogBitmap;
     *a = pts[t.x]; *b = pts[t.y]; *c = pts[t.z];
-    int ylo = min(a->y, min(b->y, c->y)), yhi = max(a->y, max(b->y, c->y));
-    *r0 = ylo >> shift;
-    *r1 = min((1 << kLogBitmap) - 1, yhi >> shift);
+    int lx = min(a->x, min(b->x, c->x)), hx = max(a->x, max(b->x, c->x));
+    int ly = min(a->y, min(b->y, c->y)), hy = max(a->y, max(b->y, c->y));
+    *x0 = lx >> shift;
+    *y0 = ly >> shift;
+    *nx = (hx >> shift) - *x0 + 1;
+    *ny = (hy >> shift) - *y0 + 1;
 }
-__global__ void bitmap_count(const int2* pts, const int3* tris, int n, int* cell_count) {
+__global__ void bbox_counts(const int2* pts, const int3* tris, int nt, long long* cnt) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+    if (t > nt) return;
+    if (t == nt) { cnt[t] = 0; return; }
     int2 a, b, c;
-    int r0, r1;
-    tri_rows(pts, tris[t], &a, &b, &c, &r0, &r1);
-    for (int r = r0; r <= r1; ++r) {
-        int c0, c1;
-        if (!row_span(a, b, c, r, &c0, &c1)) continue;
-        for (int x = c0; x <= c1; ++x) atomicAdd(&cell_count[(r << kLogBitmap) + x], 1);
-    }
+    int x0, y0, nx, ny;
+    tri_cells(pts, tris[t], &a, &b, &c, &x0, &y0, &nx, &ny);
+    cnt[t] = (long long)nx * ny;
 }
-__global__ void bitmap_emit(const int2* pts, const int3* tris, int n, int* cursor, int* list) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    int2 a, b, c;
-    int r0, r1;
-    tri_rows(pts, tris[t], &a, &b, &c, &r0, &r1);
-    for (int r = r0; r <= r1; ++r) {
-        int c0, c1;
-        if (!row_span(a, b, c, r, &c0, &c1)) continue;
-        for (int x = c0; x <= c1; ++x) list[atomicAdd(&cursor[(r << kLogBitmap) + x], 1)] = t;
+// Closed CCW triangle abc against the closed box [x0,x1] x [y0,y1] whose
+// extents overlap the triangle's bounding box: they are disjoint iff one
+// edge has the whole box strictly on its outer (right) side, tested at the
+// box corner that lies furthest to the inner side (separating axes of two
+// convex polygons: the box's axes are covered by the bounding boxes).
+__device__ __forceinline__ bool edge_separates(int2 p, int2 q, long long x0, long long y0, long long x1,
+                                               long long y1) {
+    long long dx = (long long)q.x - p.x, dy = (long long)q.y - p.y;
+    long long rx = dy < 0 ? x1 : x0, ry = dx > 0 ? y1 : y0;
+    return dx * (ry - p.y) - dy * (rx - p.x) < 0;
+}
+__device__ __forceinline__ bool tri_meets_box(int2 a, int2 b, int2 c, long long x0, long long y0, long long x1,
+                                              long long y1) {
+    return !edge_separates(a, b, x0, y0, x1, y1) && !edge_separates(b, c, x0, y0, x1, y1) &&
+           !edge_separates(c, a, x0, y0, x1, y1);
+}
+__device__ __forceinline__ int owner_of(const long long* off, int nt, long long i) {
+    int lo = 0, hi = nt;   // last t with off[t] <= i
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid;
     }
+    return lo;
+}
+__global__ void pair_test(const int2* pts, const int3* tris, int nt, const long long* off, long long npairs,
+                          int* hit) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > npairs) return;
+    if (i == npairs) { hit[i] = 0; return; }
+    int t = owner_of(off, nt, i);
+    int2 a, b, c;
+    int x0, y0, nx, ny;
+    tri_cells(pts, tris[t], &a, &b, &c, &x0, &y0, &nx, &ny);
+    long long k = i - off[t];
+    int X = x0 + (int)(k / ny), Y = y0 + (int)(k % ny);
+    const long long side = 1ll << (kLogRes - kLogBitmap);
+    hit[i] = tri_meets_box(a, b, c, X * side, Y * side, X * side + side - 1, Y * side + side - 1);
+}
+__global__ void pair_emit(const int3* tris, const int2* pts, int nt, const long long* off, long long npairs,
+                          const int* hit, const int* pos, unsigned long long* keys) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npairs || !hit[i]) return;
+    int t = owner_of(off, nt, i);
+    int2 a, b, c;
+    int x0, y0, nx, ny;
+    tri_cells(pts, tris[t], &a, &b, &c, &x0, &y0, &nx, &ny);
+    long long k = i - off[t];
+    unsigned cell = (unsigned)((x0 + (int)(k / ny)) << kLogBitmap) + (unsigned)(y0 + (int)(k % ny));
+    keys[pos[i]] = ((unsigned long long)cell << 32) | (unsigned)t;
+}
+// Sorted (cell, triangle) keys -> CSR offsets and the triangle list.
+__global__ void csr_from_keys(const unsigned long long* keys, int total, int ncell, int* offsets, int* list) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > total) return;
+    int cell = i < total ? (int)(keys[i] >> 32) : ncell;
+    int prev = i > 0 ? (int)(keys[i - 1] >> 32) : -1;
+    for (int c = prev + 1; c <= cell; ++c) offsets[c] = i;   // cells (prev, cell] start at i
+    if (i < total) list[i] = (int)(keys[i] & 0xffffffffu);
+}
+// cons[k] = (labels[a], labels[b]): the reference's reorderPoint_s4.
+__global__ void relabel_segments(int2* cons, int s, const int* labels) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= s) return;
+    int2 c = cons[k];
+    cons[k] = make_int2(labels[c.x], labels[c.y]);
 }
 
 }  // namespace
 
 double getSamplePoints(void* cubTemp, size_t cubBytes, Point2d* points, int numPoints, Point2d*& samplePoints,
                        int*& sample, int& num) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
+    bind_device();
     EventTimer tm;
     const int ncell = 1 << (2 * kLogSample);
-    int *cell_min = nullptr, *flag = nullptr;
     samplePoints = nullptr;
     sample = nullptr;
     num = 0;
-    if (cudaMalloc(&cell_min, 4 * ncell) != cudaSuccess || cudaMalloc(&flag, 4 * (ncell + 1)) != cudaSuccess ||
-        cudaMalloc(&sample, 4 * (ncell + 4)) != cudaSuccess || cudaMalloc(&samplePoints, 8 * (ncell + 4)) != cudaSuccess) {
+    if (!g_sf.scratch.ensure(4 * (2 * (size_t)ncell + 1)) || !g_out.alloc(&sample, 4 * (ncell + 4)) ||
+        !g_out.alloc(&samplePoints, 8 * (ncell + 4))) {
         cudaGetLastError();
         fprintf(stderr, "getSamplePoints: out of device memory\n");
         return -1.0;
     }
+    int* cell_min = static_cast<int*>(g_sf.scratch.p);
+    int* flag = cell_min + ncell;
     fill_ints<<<(ncell + 255) / 256, 256>>>(cell_min, INT_MAX, ncell);
     if (numPoints > 0) sample_cells<<<(numPoints + 255) / 256, 256>>>(points, numPoints, cell_min);
     sample_flags<<<(ncell + 256) / 256, 256>>>(cell_min, flag, ncell);
-    exclusive_sum(cubTemp, cubBytes, flag, flag, ncell + 1);
+    if (!exclusive_sum(cubTemp, cubBytes, flag, flag, ncell + 1)) return -1.0;
     sample_emit<<<(ncell + 255) / 256, 256>>>(points, cell_min, flag, ncell, sample, samplePoints);
     num = read_int(flag + ncell);
-    cudaFree(cell_min);
-    cudaFree(flag);
     return tm.stop();
 }
 
 double rawMeshBefore(void*, size_t, Point2d* points, int3* tris, int* sons, int& numTriangles, int numPoints) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
     EventTimer tm;
-    int nt = solve(points, numPoints, nullptr, 0, tris, nullptr, "rawMeshBefore");
+    int nt = solve_cached(points, numPoints, nullptr, 0, "rawMeshBefore");
     if (nt < 0) return -1.0;
+    copy_out(tris, nullptr, nt);
     mark_live(sons, nt);
     numTriangles = nt;
     return tm.stop();
@@ -262,9 +477,11 @@ double rawMeshBefore(void*, size_t, Point2d* points, int3* tris, int* sons, int&
 
 double rawMeshAfter(void*, size_t, Point2d* points, int3* tris, int3* adjTris, int* sons, int*, int*,
                     int& numTriangles, int numPoints) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
     EventTimer tm;
-    int nt = solve(points, numPoints, nullptr, 0, tris, adjTris, "rawMeshAfter");
+    int nt = solve_cached(points, numPoints, nullptr, 0, "rawMeshAfter");
     if (nt < 0) return -1.0;
+    copy_out(tris, adjTris, nt);
     mark_live(sons, nt);
     numTriangles = nt;
     return tm.stop();
@@ -276,28 +493,36 @@ void rawMesh(void* cubTemp, size_t cubBytes, Point2d* points, int3* tris, int3* 
 }
 
 double delaunaySample(void*, size_t, Point2d* points, int3* tris, int3* adjTris, int numPoints, int numTriangles) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
     EventTimer tm;
     if (numTriangles != 2 * (numPoints - 4) + 2) {
         fprintf(stderr, "delaunaySample: %d triangles for %d points\n", numTriangles, numPoints);
         return -1.0;
     }
-    if (solve(points, numPoints - 4, nullptr, 0, tris, adjTris, "delaunaySample") < 0) return -1.0;
+    int nt = solve_cached(points, numPoints - 4, nullptr, 0, "delaunaySample");
+    if (nt < 0) return -1.0;
+    copy_out(tris, adjTris, nt);
     return tm.stop();
 }
 
 double tryFastDelaunay(void*, size_t, Point2d* points, int3* tris, int3* adjTris, int numPoints, int) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
     EventTimer tm;
-    if (solve(points, numPoints - 4, nullptr, 0, tris, adjTris, "tryFastDelaunay") < 0) return -1.0;
+    int nt = solve_cached(points, numPoints - 4, nullptr, 0, "tryFastDelaunay");
+    if (nt < 0) return -1.0;
+    copy_out(tris, adjTris, nt);
     return tm.stop();
 }
 
 double addConstraints(void*, size_t, Point2d* points, int3* tris, int3* adjTris, int* sons, int*, int*, int2* cons,
                       int3*& newTris, int numCons, int numPoints, int, int& numNewTris) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
     EventTimer tm;
     newTris = nullptr;
     numNewTris = 0;
-    int nt = solve(points, numPoints, cons, numCons, tris, adjTris, "addConstraints");
+    int nt = solve_cached(points, numPoints, cons, numCons, "addConstraints");
     if (nt < 0) return -1.0;
+    copy_out(tris, adjTris, nt);
     mark_live(sons, nt);
     return tm.stop();
 }
@@ -310,57 +535,135 @@ double addConstraints(void* cubTemp, size_t cubBytes, Point2d* points, int3* tri
                           numPoints, numTriangles, nn);
 }
 
-double delaunayNew(void*, size_t, Point2d*& points, int3*& tris, int2* cons, int numPoints, int, int numCons) {
+// The constrained Delaunay triangulation in the reference's returned layout
+// (kernel.cu:4697-4701, 1886-2068): `points` and `tris` are replaced by new
+// buffers holding the Morton-renumbered points (corners included) and the
+// triangles over the new numbers, sorted by centroid code; the constraint
+// endpoints in `cons` are renumbered in place (reorderPoint_s4).  The new
+// buffers come from cudaMalloc and belong to the caller; the replaced ones
+// are left untouched (the reference returns them to its own pool).
+double delaunayNew(void*, size_t, Point2d*& points, int3*& tris, int2* cons, int numPoints, int numTriangles,
+                   int numCons) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
     EventTimer tm;
-    if (solve(points, numPoints - 4, cons, numCons, tris, nullptr, "delaunayNew") < 0) return -1.0;
+    const int n = numPoints - 4;
+    int nt = solve_cached(points, n, cons, numCons, "delaunayNew");
+    if (nt < 0) return -1.0;
+    if (numTriangles != nt)
+        fprintf(stderr, "delaunayNew: %d triangles given, the triangulation has %d\n", numTriangles, nt);
+    const size_t nv = (size_t)n + 4;
+    const size_t need = gcdt_reference_layout_scratch_bytes(n, nt);
+    // pooled: labels, adjacency and flags of the layout (not returned), then its scratch
+    const size_t o_adj = (4 * nv + 255) & ~size_t(255);
+    const size_t o_cf = o_adj + ((12 * (size_t)nt + 255) & ~size_t(255));
+    const size_t o_scr = o_cf + (((size_t)nt + 255) & ~size_t(255));
+    Point2d* pts_out = nullptr;
+    int3* tris_out = nullptr;
+    if (!g_sf.scratch.ensure(o_scr + need) || !g_out.alloc(&pts_out, 8 * nv) ||
+        !g_out.alloc(&tris_out, 12 * (size_t)(nt > 0 ? nt : 1))) {
+        cudaGetLastError();
+        if (pts_out) cudaFree(pts_out);
+        fprintf(stderr, "delaunayNew: out of device memory\n");
+        return -1.0;
+    }
+    char* base = static_cast<char*>(g_sf.scratch.p);
+    int* labels = reinterpret_cast<int*>(base);
+    gcdt_status rc = gcdt_reference_layout(
+        reinterpret_cast<const int32_t*>(points), n, static_cast<const int32_t*>(g_sf.c_tris.p),
+        static_cast<const int32_t*>(g_sf.c_adj.p), static_cast<const uint8_t*>(g_sf.c_cf.p), nt,
+        reinterpret_cast<int32_t*>(pts_out), labels, reinterpret_cast<int32_t*>(tris_out),
+        reinterpret_cast<int32_t*>(base + o_adj), reinterpret_cast<uint8_t*>(base + o_cf), base + o_scr, need, nullptr);
+    if (rc != GCDT_OK) {
+        cudaFree(pts_out);
+        cudaFree(tris_out);
+        fprintf(stderr, "delaunayNew: %s\n", gcdt_status_string(rc));
+        return -1.0;
+    }
+    if (numCons > 0 && cons) relabel_segments<<<(numCons + 255) / 256, 256>>>(cons, numCons, labels);
+    points = pts_out;
+    tris = tris_out;
     return tm.stop();
 }
 
 double filterTriangles(void* cubTemp, size_t cubBytes, int3* tris, int3* newTris, int3* adjTris, int3* newAdjTris,
                        int* sons, int& numTriangles) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
+    bind_device();
     EventTimer tm;
     int n = numTriangles;
-    int* off = nullptr;
-    if (cudaMalloc(&off, 4 * ((size_t)n + 1)) != cudaSuccess) {
-        cudaGetLastError();
+    if (!g_sf.scratch.ensure(4 * ((size_t)n + 1))) {
         fprintf(stderr, "filterTriangles: out of device memory\n");
         return -1.0;
     }
+    int* off = static_cast<int*>(g_sf.scratch.p);
     live_flags<<<(n + 256) / 256, 256>>>(sons, off, n);
-    exclusive_sum(cubTemp, cubBytes, off, off, n + 1);
+    if (!exclusive_sum(cubTemp, cubBytes, off, off, n + 1)) return -1.0;
     if (n > 0) compact_tris<<<(n + 255) / 256, 256>>>(tris, newTris, adjTris, newAdjTris, sons, off, n);
     numTriangles = read_int(off + n);
-    cudaFree(off);
     return tm.stop();
 }
 
 double getBitmap(void* cubTemp, size_t cubBytes, Point2d* points, int3* tris, int*& bitmapOffsets, int*& bitmapTris,
                  int numTriangles) {
+    std::lock_guard<std::mutex> lk(g_sf.mu);
+    bind_device();
     EventTimer tm;
     const int ncell = 1 << (2 * kLogBitmap);
-    int* cursor = nullptr;
+    const int nt = numTriangles > 0 ? numTriangles : 0;
     bitmapOffsets = nullptr;
     bitmapTris = nullptr;
-    if (cudaMalloc(&bitmapOffsets, 4 * ((size_t)ncell + 1)) != cudaSuccess ||
-        cudaMalloc(&cursor, 4 * ((size_t)ncell + 1)) != cudaSuccess) {
-        cudaGetLastError();
+    // bounding-box cells per triangle and their scan (64-bit: a triangle at
+    // a box corner may span most of the grid)
+    if (!g_sf.scratch.ensure(8 * ((size_t)nt + 1))) {
         fprintf(stderr, "getBitmap: out of device memory\n");
         return -1.0;
     }
-    cudaMemset(bitmapOffsets, 0, 4 * ((size_t)ncell + 1));
-    if (numTriangles > 0)
-        bitmap_count<<<(numTriangles + 127) / 128, 128>>>(points, tris, numTriangles, bitmapOffsets);
-    exclusive_sum(cubTemp, cubBytes, bitmapOffsets, bitmapOffsets, ncell + 1);
-    int total = read_int(bitmapOffsets + ncell);
-    if (cudaMalloc(&bitmapTris, 4 * ((size_t)total + 1)) != cudaSuccess) {
-        cudaGetLastError();
-        cudaFree(cursor);
+    long long* off = static_cast<long long*>(g_sf.scratch.p);
+    bbox_counts<<<(nt + 256) / 256, 256>>>(points, tris, nt, off);
+    size_t need = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, off, off, nt + 1);
+    if (!g_sf.scratch2.ensure(need + 256)) return -1.0;
+    cub::DeviceScan::ExclusiveSum(static_cast<char*>(g_sf.scratch2.p) + 256, need, off, off, nt + 1);
+    long long npairs = 0;
+    cudaMemcpy(&npairs, off + nt, sizeof(long long), cudaMemcpyDeviceToHost);
+    if (npairs > (long long)INT_MAX - 1) {
+        fprintf(stderr, "getBitmap: %lld triangle-cell pairs\n", npairs);
+        return -1.0;
+    }
+    // the exact test of every pair, and each hit's position
+    const size_t o_pos = (4 * ((size_t)npairs + 1) + 255) & ~size_t(255);
+    if (!g_sf.pairs.ensure(2 * o_pos)) {
         fprintf(stderr, "getBitmap: out of device memory\n");
         return -1.0;
     }
-    cudaMemcpy(cursor, bitmapOffsets, 4 * ((size_t)ncell + 1), cudaMemcpyDeviceToDevice);
-    if (numTriangles > 0)
-        bitmap_emit<<<(numTriangles + 127) / 128, 128>>>(points, tris, numTriangles, cursor, bitmapTris);
-    cudaFree(cursor);
+    int* flag = static_cast<int*>(g_sf.pairs.p);
+    int* pos = reinterpret_cast<int*>(static_cast<char*>(g_sf.pairs.p) + o_pos);
+    pair_test<<<(unsigned)((npairs + 256) / 256), 256>>>(points, tris, nt, off, npairs, flag);
+    cub::DeviceScan::ExclusiveSum(nullptr, need, flag, pos, (int)npairs + 1);
+    if (!g_sf.scratch2.ensure(need + 256)) return -1.0;
+    cub::DeviceScan::ExclusiveSum(static_cast<char*>(g_sf.scratch2.p) + 256, need, flag, pos, (int)npairs + 1);
+    const int total = read_int(pos + npairs);
+    // (cell, triangle) keys sorted: cells in order, triangles ascending in each
+    const size_t o_k1 = (8 * ((size_t)total + 1) + 255) & ~size_t(255);
+    if (!g_sf.keys.ensure(2 * o_k1) || !g_out.alloc(&bitmapOffsets, 4 * ((size_t)ncell + 1)) ||
+        !g_out.alloc(&bitmapTris, 4 * ((size_t)total + 1))) {
+        cudaGetLastError();
+        if (bitmapOffsets) cudaFree(bitmapOffsets);
+        bitmapOffsets = nullptr;
+        fprintf(stderr, "getBitmap: out of device memory\n");
+        return -1.0;
+    }
+    unsigned long long* k0 = static_cast<unsigned long long*>(g_sf.keys.p);
+    unsigned long long* k1 = reinterpret_cast<unsigned long long*>(static_cast<char*>(g_sf.keys.p) + o_k1);
+    pair_emit<<<(unsigned)((npairs + 255) / 256), 256>>>(tris, points, nt, off, npairs, flag, pos, k0);
+    if (total > 0) {
+        cub::DoubleBuffer<unsigned long long> dk(k0, k1);
+        cub::DeviceRadixSort::SortKeys(nullptr, need, dk, total, 0, 2 * kLogBitmap + 32);
+        if (!g_sf.scratch2.ensure(need + 256)) return -1.0;
+        cub::DeviceRadixSort::SortKeys(static_cast<char*>(g_sf.scratch2.p) + 256, need, dk, total, 0,
+                                       2 * kLogBitmap + 32);
+        k0 = dk.Current();
+    }
+    csr_from_keys<<<(total + 256) / 256, 256>>>(k0, total, ncell, bitmapOffsets, bitmapTris);
     return tm.stop();
 }

@@ -85,6 +85,7 @@ gcdt_status gcdt_triangulate(gcdt_context* ctx, const int32_t* d_points, int32_t
                              int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,
                              int32_t* n_tris, void* stream);
 
+
 /* The same solve, enqueued on `stream` without waiting for it: returns once
    the work is queued (GCDT_OK), or with the argument / capacity error.  The
    solve's own status (bad input found on the device, crossing constraints,
@@ -141,6 +142,12 @@ typedef struct {
     int32_t narrow_active;
 } gcdt_tuning;
 gcdt_status gcdt_set_tuning(gcdt_context* ctx, const gcdt_tuning* tuning);   /* NULL: the defaults */
+/* Blocks of the persistent stage kernel's launch for ctx's solves (0, the
+   default: every co-resident block, one per SM; larger values are capped
+   there).  Fewer blocks leave SMs to other work, so several contexts can
+   solve at once; the result does not depend on it.  No counterpart in the
+   reference. */
+gcdt_status gcdt_set_grid_blocks(gcdt_context* ctx, int32_t blocks);
 gcdt_status gcdt_get_tuning(const gcdt_context* ctx, gcdt_tuning* tuning);
 /* Solve the given problem under each of a fixed set of schedules (the
    defaults, other level strides, two-level schedules, other carries), best
@@ -162,6 +169,12 @@ gcdt_status gcdt_autotune(gcdt_context* ctx, const int32_t* d_points, int32_t n,
    whose waits are unbounded. */
 gcdt_status gcdt_probe_barrier(int device, int32_t blocks, int32_t absent_block, uint32_t spin_limit,
                                int32_t* timed_out);
+/* Cost of the persistent kernel's grid barrier on `device`: a grid shaped
+   like the stage kernel's (one block per co-resident slot) passes `rounds`
+   barriers with no work between them; *us_per_barrier receives the
+   CUDA-event time per barrier in microseconds.  Every wait is bounded.  No
+   counterpart in the reference. */
+gcdt_status gcdt_time_barriers(int device, int32_t rounds, double* us_per_barrier);
 
 /* Per-phase profile of the last solve on ctx: SM cycles spent in each phase
    kind of the persistent stage kernel (measured by block 0, barrier wait
@@ -169,6 +182,16 @@ gcdt_status gcdt_probe_barrier(int device, int32_t blocks, int32_t absent_block,
    (names: gcdt_phase_name), or -1 on bad arguments.  Counters of the
    reference's per-stage cudaEvent printouts (e.g. rawMesh.cu:1008-1031). */
 int32_t gcdt_get_phase_profile(const gcdt_context* ctx, int64_t* cycles, int64_t* counts, int32_t max_kinds);
+/* Balance of the grid-wide phases of the last solve (no counterpart in the
+   reference): per phase kind, the sum over its runs of the longest block's
+   work time (wmax) and of all blocks' work times (wsum), in SM cycles, the
+   work time of a block being the time from the phase's start to its arrival
+   at the phase's barrier.  wmax against the phase's cycles from
+   gcdt_get_phase_profile shows the barrier's share, wsum / blocks against
+   wmax the imbalance; *blocks receives the block count.  Returns the number
+   of kinds written (or -1). */
+int32_t gcdt_get_phase_balance(const gcdt_context* ctx, int64_t* wmax, int64_t* wsum, int64_t* blocks,
+                               int32_t max_kinds);
 const char* gcdt_phase_name(int32_t kind);
 
 /* Exact predicates on device, for parity tests.  d_quads: 8 int32 per case
@@ -272,10 +295,11 @@ double gcdt_batch_last_ms(const gcdt_batch* batch);
    workspace gcdt_workspace_bytes(n, s) from a lane), packs queued requests
    into batches on `lanes` concurrent streams as lanes free up (continuous
    batching: work of requests that arrive while others run overlaps theirs
-   on the device), runs requests of at least big_request_points points one at
-   a time on the whole GPU from a second worker on a high-priority stream,
-   concurrently with the lanes, and keeps every result resident until it is
-   fetched or released.  Submission copies the caller's host arrays; all calls are
+   on the device), runs requests of at least big_request_points points
+   through the single-solve path from big_workers worker threads on
+   high-priority streams (one on the whole GPU, or several on a share of the
+   SMs each), concurrently with the lanes, and keeps every result resident
+   until it is fetched or released.  Submission copies the caller's host arrays; all calls are
    thread-safe. */
 typedef struct gcdt_server gcdt_server;
 typedef struct {
@@ -288,6 +312,10 @@ typedef struct {
     int64_t big_request_points;     /* at least this many points: the whole-GPU single solve */
     int64_t max_request_points;
     int64_t max_request_segments;
+    int32_t big_workers;            /* 0 or 1: one worker for large requests on the whole GPU; k > 1:
+                                       k workers, each solving on 1/k of the SMs, so k large
+                                       requests run at once */
+    int32_t reserved;               /* 0 */
 } gcdt_server_config;
 typedef struct {
     int64_t submitted, completed, failed, batches, big_solves, queued;
@@ -342,12 +370,12 @@ int gcdt_text_save(const char* path, const int32_t* points_xy, int64_t n_points,
    not leave a stale address); as that is the call's set-up, make every call
    before any stream capture starts on the device.  The call returns once the
    solve has finished.  Problems needing more workspace than the array
-   (gcdt_workspace_bytes(n, s) > GCDT_NOALLOC_WORKSPACE_BYTES, about 100,000
+   (gcdt_workspace_bytes(n, s) > GCDT_NOALLOC_WORKSPACE_BYTES, about 120,000
    points) return GCDT_OOM without touching the device.  Calls share the
    array: calls that overlap on the GPU race and corrupt each other, so
    serialize them.  Inputs and outputs are as for gcdt_triangulate; the
    caller passes the device buffers, and the call allocates nothing. */
-#define GCDT_NOALLOC_WORKSPACE_BYTES ((size_t)32 << 20)
+#define GCDT_NOALLOC_WORKSPACE_BYTES ((size_t)40 << 20)
 gcdt_status gcdt_triangulate_noalloc(const int32_t* d_points, int32_t n,
                                      const int32_t* d_segments, int32_t s,
                                      int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,

@@ -110,3 +110,14 @@ def test_limit_arguments_are_checked_without_a_device():
     out = ctypes.c_int32(0)
     assert g.STATUS[L.gcdt_probe_barrier(0, 0, 0, 16, ctypes.byref(out))] == "BAD_INPUT"
     assert g.STATUS[L.gcdt_probe_barrier(0, 4, 0, 0, ctypes.byref(out))] == "BAD_INPUT"
+
+
+@pytest.mark.gpu
+def test_grid_barrier_cost_is_measured_and_bounded():
+    """The persistent kernel's grid barrier, alone in a loop on a grid shaped
+    like the stage kernel's: every wait completes (bounded polls) and one
+    barrier costs a few microseconds, so a flip sub-round's three barriers
+    are a small part of its time."""
+    us = g.time_barriers(rounds=4096)
+    print("grid barrier: %.2f us" % us)
+    assert 0 < us < 50

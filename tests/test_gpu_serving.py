@@ -70,3 +70,50 @@ def test_admission_waits_for_memory():
         assert len(t) == 2 * len(reqs[i][0]) + 2
     assert sv.stats()["completed"] == len(reqs)
     sv.close()
+
+
+def _overlap(a, b):
+    return max(a[0], b[0]) < min(a[1], b[1])
+
+
+def test_work_of_different_requests_overlaps_on_the_device():
+    """Continuous batching runs requests' work side by side: two small
+    requests in different batches (so on two lanes), a small request and a
+    large one (a lane and a single-solve worker), and two large requests
+    (two workers, each on half of the SMs) are in flight at the same time,
+    by the server's own start/completion times; every result equals the
+    single solve."""
+    small = _requests(36, 1300, cap=20_000)
+    big = [g.generate(g.GEN_SERVING_REQUEST, 1400 + i, 150_000) for i in range(4)]
+    sv = g.Server(memory_budget_bytes=24 << 30, lanes=3, max_batch_instances=4, max_batch_points=80_000,
+                  max_batch_segments=8_000, big_request_points=100_000, max_request_points=200_000,
+                  max_request_segments=10_000, big_workers=2)
+    order = []
+    for i in range(len(small)):
+        order.append(("s", i))
+        if i % 9 == 0:
+            order.append(("b", i // 9))
+    ids = {}
+    for kind, i in order:
+        ids[(kind, i)] = sv.submit(*(small[i] if kind == "s" else big[i]))
+    times = {}
+    for key, rid in ids.items():
+        done, rc = sv.wait(rid)
+        assert done and rc == 0
+        sub, start, end = sv.times(rid)
+        times[key] = (start, end)
+    smalls = [times[("s", i)] for i in range(len(small))]
+    bigs = [times[("b", i)] for i in range(len(big))]
+    assert any(_overlap(a, b) for k, a in enumerate(smalls) for b in smalls[k + 1:] if a[0] != b[0])
+    assert any(_overlap(a, b) for a in smalls for b in bigs)
+    assert any(_overlap(a, b) for k, a in enumerate(bigs) for b in bigs[k + 1:])
+    single = g.Triangulator(200_000, 10_000)
+    for (kind, i), rid in ids.items():
+        xy, cons = small[i] if kind == "s" else big[i]
+        t, a, c = sv.fetch(rid, len(xy))
+        st, sa, sc = single.triangulate_host(xy, cons)
+        assert np.array_equal(canonical_with_flags(t, c), canonical_with_flags(st, sc))
+    st = sv.stats()
+    assert st["big_solves"] == len(big) and st["batches"] >= 3 and st["failed"] == 0
+    single.close()
+    sv.close()
