@@ -58,6 +58,7 @@ class Stats(ctypes.Structure):
         ("flip_subrounds", ctypes.c_int64), ("flips", ctypes.c_int64),
         ("constraint_rounds", ctypes.c_int64), ("host_syncs", ctypes.c_int64),
         ("kernel_launches", ctypes.c_int64), ("device_ms", ctypes.c_double),
+        ("stage_ms", ctypes.c_double),
     ]
 
     def as_dict(self):

@@ -22,6 +22,9 @@ namespace gcdt {
 #ifndef GCDT_PERSIST_MINB
 #define GCDT_PERSIST_MINB 1
 #endif
+#ifndef GCDT_WARP_DYNAMIC
+#define GCDT_WARP_DYNAMIC 0
+#endif
 constexpr int kPersistBlock = GCDT_PERSIST_BLOCK;   // 512: one block per SM (128 registers per thread)
 constexpr int kPersistMinBlocks = GCDT_PERSIST_MINB;
 
@@ -39,6 +42,7 @@ struct GridExec {
     static constexpr int kSnapWords = 12;   // 96 bytes: status..cur_scr
     unsigned long long* snap;                // shared memory, kSnapWords entries
     unsigned spin_limit = 1u << 24;          // polls before a barrier wait gives up
+    int* work = nullptr;                     // shared memory: the block's next item (dynamic phases)
 
     __device__ void take_snapshot() {
         volatile unsigned long long* src = reinterpret_cast<volatile unsigned long long*>(cnt);
@@ -87,7 +91,9 @@ struct GridExec {
     __device__ void phase(int k, const Ctx& c, long long count) {
         const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
         long long t0 = threadIdx.x == 0 ? clock64() : 0;
-        if (!(word(&cnt->status) & ST_BARRIER)) {
+        if (!(word(&cnt->status) & ST_BARRIER) && work && GCDT_WARP_DYNAMIC) {
+            dynamic_items(k, c, count);
+        } else if (!(word(&cnt->status) & ST_BARRIER)) {
             long long stride = (long long)gridDim.x * blockDim.x;
             long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
             // latency-bound passes: two items per thread and trip (i, i + stride)
@@ -118,6 +124,37 @@ struct GridExec {
             cnt->wcur_sum[slot] = 0;
         }
     }
+    // Items of a phase as contiguous per-block ranges that the block's warps
+    // take in chunks from a shared-memory counter: a warp that finishes early
+    // takes more, so the block's warps end together.
+    __device__ void dynamic_items(int k, const Ctx& c, long long count) {
+        const long long per = (count + gridDim.x - 1) / gridDim.x;
+        const long long b0 = (long long)blockIdx.x * per;
+        const long long b1 = b0 + per < count ? b0 + per : count;
+        if (threadIdx.x == 0) *work = 0;
+        __syncthreads();
+        const bool pair = k == K_FLIP_CHECK || k == K_FLIP_DO || k == K_FLIP_FIX;
+        const int chunk = pair ? 64 : 32;
+        const int lane = threadIdx.x & 31;
+        for (;;) {
+            int off = 0;
+            if (lane == 0) off = atomicAdd(work, chunk);
+            off = __shfl_sync(0xffffffffu, off, 0);
+            const long long base = b0 + off;
+            if (base >= b1) break;
+            const long long i0 = base + lane;
+            if (i0 >= b1) continue;
+            if (pair) {
+                const long long i1 = i0 + 32;
+                const int k1 = i1 < b1 ? (int)i1 : -1;
+                if (k == K_FLIP_CHECK) body_flip_check_pair(c, (int)i0, k1);
+                else if (k == K_FLIP_DO) body_flip_do_pair(c, (int)i0, k1);
+                else body_flip_fix_pair(c, (int)i0, k1);
+            } else {
+                dispatch(k, c, (int)i0);
+            }
+        }
+    }
     // Values read after a barrier come from the block's snapshot.
     __device__ unsigned long long cursor(unsigned long long* p) {
         size_t off = (size_t)((char*)p - (char*)cnt);
@@ -146,7 +183,27 @@ struct BlockExec {
     static constexpr bool kCanNarrow = false;
     Counters* cnt;
     __device__ void phase(int k, const Ctx& c, long long count) {
-        for (long long i = threadIdx.x; i < count; i += blockDim.x) dispatch(k, c, (int)i);
+        const long long stride = blockDim.x;
+        long long i = threadIdx.x;
+        // the latency-bound flip passes: two items per thread and trip, as
+        // on the grid, so a queue of up to two blocks' worth is one trip
+#ifndef GCDT_BLOCK_PAIRS
+#define GCDT_BLOCK_PAIRS 1
+#endif
+        if (!GCDT_BLOCK_PAIRS) {
+            for (; i < count; i += stride) dispatch(k, c, (int)i);
+        } else if (k == K_FLIP_CHECK) {
+            for (; i < count; i += 2 * stride)
+                body_flip_check_pair(c, (int)i, i + stride < count ? (int)(i + stride) : -1);
+        } else if (k == K_FLIP_DO) {
+            for (; i < count; i += 2 * stride)
+                body_flip_do_pair(c, (int)i, i + stride < count ? (int)(i + stride) : -1);
+        } else if (k == K_FLIP_FIX) {
+            for (; i < count; i += 2 * stride)
+                body_flip_fix_pair(c, (int)i, i + stride < count ? (int)(i + stride) : -1);
+        } else {
+            for (; i < count; i += stride) dispatch(k, c, (int)i);
+        }
         __syncthreads();
     }
     __device__ unsigned long long cursor(unsigned long long* p) { return *(volatile unsigned long long*)p; }

@@ -40,7 +40,9 @@ static_assert(offsetof(Counters, cur_scr) + 8 <= GridExec::kSnapWords * 8, "curs
 
 __global__ void __launch_bounds__(kPersistBlock, kPersistMinBlocks) gcdt_stages(Ctx c) {
     __shared__ unsigned long long snap[GridExec::kSnapWords];
+    __shared__ int work;
     GridExec ex{c.cnt, gridDim.x, snap};
+    ex.work = &work;
     if (threadIdx.x == 0) ex.take_snapshot();
     __syncthreads();
     run_stages(ex, c);
@@ -99,6 +101,7 @@ struct DeviceBackend {
     // All rounds run in one cooperative launch sized to the co-resident
     // block count, so every block is resident and the grid barrier is safe.
     int grid_limit = 0;   // at most this many blocks (0: no limit)
+    cudaEvent_t ev_stage0 = nullptr, ev_stage1 = nullptr;   // recorded around the stage launch when set
     void stages(const Ctx& c) {
         if (err != cudaSuccess) return;
         int dev = 0, sms = 0, per_sm = 0;
@@ -109,36 +112,11 @@ struct DeviceBackend {
         int blocks = sms * per_sm;
         if (grid_limit > 0 && grid_limit < blocks) blocks = grid_limit;
         Ctx cc = c;
-#ifdef GCDT_PIN_POINTS
-        // measurement variant: the sorted point array as a persisting L2 window
-        int max_win = 0, max_persist = 0;
-        note(cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, dev));
-        note(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
-        size_t win = 8 * ((size_t)c.n + 4);
-        if (win > (size_t)max_win) win = (size_t)max_win;
-        if (win > (size_t)max_persist) win = (size_t)max_persist;
-        note(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, win));
-        cudaLaunchConfig_t lc = {};
-        lc.gridDim = dim3(blocks);
-        lc.blockDim = dim3(kPersistBlock);
-        lc.stream = st;
-        cudaLaunchAttribute at[2];
-        at[0].id = cudaLaunchAttributeCooperative;
-        at[0].val.cooperative = 1;
-        at[1].id = cudaLaunchAttributeAccessPolicyWindow;
-        at[1].val.accessPolicyWindow.base_ptr = c.P;
-        at[1].val.accessPolicyWindow.num_bytes = win;
-        at[1].val.accessPolicyWindow.hitRatio = 1.0f;
-        at[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-        at[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-        lc.attrs = at;
-        lc.numAttrs = 2;
-        note(cudaLaunchKernelEx(&lc, gcdt_stages, cc));
-#else
         void* args[] = {&cc};
+        if (ev_stage0) note(cudaEventRecord(ev_stage0, st));
         note(cudaLaunchCooperativeKernel((const void*)gcdt_stages, dim3(blocks), dim3(kPersistBlock),
                                          args, 0, st));
-#endif
+        if (ev_stage1) note(cudaEventRecord(ev_stage1, st));
         launches++;
     }
     void read(Counters* h) {
@@ -201,6 +179,7 @@ struct gcdt_context {
     char* arena = nullptr;
     Counters* hcnt = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evs0 = nullptr, evs1 = nullptr;   // around the stage kernel
     gcdt_stats stats{};
     // the solve enqueued by gcdt_triangulate_async, until gcdt_wait
     bool pending = false;
@@ -252,7 +231,8 @@ extern "C" gcdt_status gcdt_create(gcdt_context** out, int device, int64_t max_p
         return GCDT_OOM;
     }
     if (cudaMallocHost(&ctx->hcnt, sizeof(Counters)) != cudaSuccess ||
-        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaEventCreate(&ctx->evs0) != cudaSuccess || cudaEventCreate(&ctx->evs1) != cudaSuccess) {
         cudaGetLastError();
         gcdt_destroy(ctx);
         return GCDT_CUDA_ERROR;
@@ -269,6 +249,8 @@ extern "C" void gcdt_destroy(gcdt_context* ctx) {
     if (ctx->hcnt) cudaFreeHost(ctx->hcnt);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->evs0) cudaEventDestroy(ctx->evs0);
+    if (ctx->evs1) cudaEventDestroy(ctx->evs1);
     delete ctx;
 }
 
@@ -303,6 +285,10 @@ gcdt_status enqueue(gcdt_context* ctx, const int32_t* d_points, int32_t n, const
     bk.sort_tmp = ctx->arena + plan.o_sort_tmp;
     bk.sort_bytes = plan.sort_temp_bytes;
     bk.grid_limit = ctx->grid_blocks;
+    bk.ev_stage0 = ctx->evs0;
+    bk.ev_stage1 = ctx->evs1;
+    bk.note(cudaEventRecord(ctx->evs0, bk.st));   // both stage events exist even if the launch is skipped
+    bk.note(cudaEventRecord(ctx->evs1, bk.st));
     bk.note(cudaEventRecord(ctx->ev0, bk.st));
     enqueue_solve(bk, c);
     bk.note(cudaMemcpyAsync(ctx->hcnt, c.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, bk.st));
@@ -340,8 +326,9 @@ extern "C" gcdt_status gcdt_wait(gcdt_context* ctx, int32_t* n_tris) {
         cudaGetLastError();
         bits |= ST_CUDA;
     }
-    float ms = 0.f;
+    float ms = 0.f, sms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    cudaEventElapsedTime(&sms, ctx->evs0, ctx->evs1);
     const int32_t n = ctx->pend_n;
     gcdt_stats& S = ctx->stats;
     S.n_points = n;
@@ -354,6 +341,7 @@ extern "C" gcdt_status gcdt_wait(gcdt_context* ctx, int32_t* n_tris) {
     S.host_syncs = 1;
     S.kernel_launches = ctx->pend_launches;
     S.device_ms = ms;
+    S.stage_ms = sms;
     gcdt_status rc = map_status(bits);
     if (rc == GCDT_OK && n_tris) *n_tris = 2 * n + 2;
     return rc;

@@ -64,6 +64,7 @@ typedef struct {
     int64_t host_syncs;
     int64_t kernel_launches;
     double device_ms;          /* CUDA-event time of the whole solve */
+    double stage_ms;           /* CUDA-event time of the persistent stage kernel alone */
 } gcdt_stats;
 
 /* Largest point count a context accepts (triangle ids must fit 29 bits). */
