@@ -376,7 +376,7 @@ int gcdt_text_save(const char* path, const int32_t* points_xy, int64_t n_points,
    array: calls that overlap on the GPU race and corrupt each other, so
    serialize them.  Inputs and outputs are as for gcdt_triangulate; the
    caller passes the device buffers, and the call allocates nothing. */
-#define GCDT_NOALLOC_WORKSPACE_BYTES ((size_t)40 << 20)
+#define GCDT_NOALLOC_WORKSPACE_BYTES ((size_t)32 << 20)
 gcdt_status gcdt_triangulate_noalloc(const int32_t* d_points, int32_t n,
                                      const int32_t* d_segments, int32_t s,
                                      int32_t* d_tris, int32_t* d_adj, uint8_t* d_cflags,

@@ -52,7 +52,7 @@ def test_noalloc_equals_context_entry_point_twice_in_a_row():
     inputs = [g.generate(g.GEN_SMALL, 1),                     # 100,512 points + 512 segments
               g.generate(g.GEN_BATCH_INSTANCE, 3, 20000)]     # a different, smaller instance
     for xy, cons in inputs:
-        assert g.workspace_bytes(len(xy), len(cons)) <= (40 << 20)
+        assert g.workspace_bytes(len(xy), len(cons)) <= (32 << 20)
     tri = g.Triangulator(max_points=max(len(x) for x, _ in inputs),
                          max_segments=max(len(c) for _, c in inputs))
     expected = [tri.triangulate_host(xy, cons) for xy, cons in inputs]
@@ -67,8 +67,8 @@ def test_noalloc_equals_context_entry_point_twice_in_a_row():
 def test_noalloc_rejects_problems_beyond_the_static_workspace():
     import torch
     f = _noalloc()
-    n = 400000          # needs ~140 MB of workspace, more than the 40 MiB array
-    assert g.workspace_bytes(n, 0) > (40 << 20)
+    n = 400000          # needs ~110 MB of workspace, more than the 32 MiB array
+    assert g.workspace_bytes(n, 0) > (32 << 20)
     dummy = torch.zeros(16, dtype=torch.int32, device="cuda")
     nt = ctypes.c_int32(0)
     ptr = ctypes.c_void_p(dummy.data_ptr())
