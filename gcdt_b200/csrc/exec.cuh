@@ -137,29 +137,34 @@ struct GridExec {
     // being chunk b + j * blocks of the phase (the grid-stride interleave);
     // the block's warps take its chunks in turn from a shared-memory
     // counter, so a warp that finishes early takes more.
+    __device__ int take_chunk() {
+        int j = 0;
+        if ((threadIdx.x & 31) == 0) j = atomicAdd(work, 1);
+        return __shfl_sync(0xffffffffu, j, 0);
+    }
     __device__ void dynamic_items(int k, const Ctx& c, long long count) {
         if (threadIdx.x == 0) *work = 0;
         __syncthreads();
         const bool pair = k == K_FLIP_CHECK || k == K_FLIP_DO || k == K_FLIP_FIX;
         const long long chunk = pair ? 64 : 32;
         const int lane = threadIdx.x & 31;
+        int j = take_chunk();
         for (;;) {
-            int j = 0;
-            if (lane == 0) j = atomicAdd(work, 1);
-            j = __shfl_sync(0xffffffffu, j, 0);
             const long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * chunk;
             if (base >= count) break;
             const long long i0 = base + lane;
-            if (i0 >= count) continue;
-            if (pair) {
-                const long long i1 = i0 + 32;
-                const int k1 = i1 < count ? (int)i1 : -1;
-                if (k == K_FLIP_CHECK) body_flip_check_pair(c, (int)i0, k1);
-                else if (k == K_FLIP_DO) body_flip_do_pair(c, (int)i0, k1);
-                else body_flip_fix_pair(c, (int)i0, k1);
-            } else {
-                dispatch(k, c, (int)i0);
+            if (i0 < count) {
+                if (pair) {
+                    const long long i1 = i0 + 32;
+                    const int k1 = i1 < count ? (int)i1 : -1;
+                    if (k == K_FLIP_CHECK) body_flip_check_pair(c, (int)i0, k1);
+                    else if (k == K_FLIP_DO) body_flip_do_pair(c, (int)i0, k1);
+                    else body_flip_fix_pair(c, (int)i0, k1);
+                } else {
+                    dispatch(k, c, (int)i0);
+                }
             }
+            j = take_chunk();
         }
     }
     // Values read after a barrier come from the block's snapshot.

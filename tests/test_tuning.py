@@ -93,3 +93,22 @@ def test_tuning_is_validated_without_a_device():
     assert g.STATUS[L.gcdt_set_tuning(None, None)] == "BAD_INPUT"
     assert g.STATUS[L.gcdt_get_tuning(None, None)] == "BAD_INPUT"
     assert g.STATUS[L.gcdt_autotune(None, None, 0, None, 0, None, None, None, 1, None, None)] == "BAD_INPUT"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("blocks", [1, 37, 100])
+def test_grid_share_gives_the_same_bytes(blocks):
+    """gcdt_set_grid_blocks: a context whose persistent kernel runs on a
+    share of the SMs (as the server's large-request workers do) returns the
+    same bytes as one on the whole GPU: the phases' results do not depend
+    on how their items are spread over blocks."""
+    xy, cons = g.generate(g.GEN_SCALE, 6, 200000, 8, 40)
+    full = g.Triangulator(max_points=len(xy), max_segments=len(cons))
+    part = g.Triangulator(max_points=len(xy), max_segments=len(cons))
+    part.set_grid_blocks(blocks)
+    a = full.triangulate_host(xy, cons)
+    b = part.triangulate_host(xy, cons)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    full.close()
+    part.close()
