@@ -3,7 +3,7 @@
 // The reference has no batched mode (kernel.cu:5332-5466 triangulates one
 // point set per process).  Here one call triangulates thousands of
 // independent instances of uneven size:
-//   1. one kernel computes the Morton key of every point of every instance;
+//   1. one kernel computes the Hilbert key of every point of every instance;
 //   2. one segmented radix sort orders each instance's points;
 //   3. one kernel with one block per instance runs the whole solve of that
 //      instance -- set-up, insertion rounds, flip sub-rounds, constraint
@@ -60,7 +60,7 @@ __global__ void gcdt_batch_keys(const int2* xy, const int* offs, int ninst, int 
     }
     int2 p = xy[g];
     if (p.x < 1 || p.y < 1 || p.x > kBoxMax - 1 || p.y > kBoxMax - 1) atomicOr(&desc[lo].status, ST_BAD_INPUT);
-    keys[g] = morton60(p);
+    keys[g] = sort_key60(p);
     vals[g] = g - offs[lo];
 }
 

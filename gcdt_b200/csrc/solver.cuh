@@ -3,7 +3,7 @@
 // kernel with its grid executor from exec.cuh).
 //
 // Phases (reference stage it replaces, yingtix/gCDT):
-//   0  Morton keys, radix sort, gather: points in spatial order
+//   0  Hilbert keys, radix sort, gather: points in spatial order
 //      (kernel.cu:1966-2019 reorderPoint, there applied before the flip stage)
 //   1  insertion rounds: every uninserted point votes for its triangle, one
 //      winner per triangle splits it (1->3, or 2->4 on an edge), adjacency is
@@ -89,7 +89,7 @@ __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     c.vt = (int*)(base + p.o_vt);
     c.lvl = (unsigned char*)(base + p.o_lvl);
     c.cnt = (Counters*)(base + p.o_cnt);
-    // three levels: every 512th point of the Morton order plus all segment
+    // three levels: every 512th point of the curve order plus all segment
     // endpoints, then every 8th, then the rest
     c.nlevels = 3;
     c.stride[0] = 512; c.stride[1] = 8; c.stride[2] = 1; c.stride[3] = 1;
@@ -367,7 +367,7 @@ GCDT_HD int run_stages(EX& ex, Ctx c) {
     return rc;
 }
 
-// Host part: clear the per-solve arrays, Morton sort, gather, levels and
+// Host part: clear the per-solve arrays, key sort, gather, levels and
 // segment set-up, then hand over to the stages (one persistent kernel on the
 // GPU).  Everything is enqueued on the backend's stream without waiting:
 // errors found by the set-up kernels make the stage kernel stop at once.
