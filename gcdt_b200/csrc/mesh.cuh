@@ -6,8 +6,11 @@
 // Layout in HBM (structure of arrays, one row per point or triangle):
 //   P[v]      int2   point v in space-filling-curve order; corners at N..N+3
 //   perm[v]   int    input index of sorted point v (corners map to N+k)
-//   tri[2t]   int4   TV: (v0, v1, v2, cflags) -- CCW vertices, bit k of .w set
-//                    when the edge opposite v_k is a constraint edge
+//   tri[2t]   int4   TV: (v0, v1, v2, w) -- CCW vertices; w bit k set when the
+//                    edge opposite v_k is a constraint edge (k < 3), bit 3 the
+//                    triangle's side of its last flip, bits 4.. the flip
+//                    sub-round of that flip (0: made by a split or a
+//                    constraint flip)
 //   tri[2t+1] int4   TA: (a0, a1, a2, -)  a_k = 4*n + j: neighbour n across the
 //                    edge opposite v_k, which is opposite slot j in n; -1 = box;
 //                    .w = the insertion round that last changed the triangle
@@ -121,7 +124,6 @@ struct Ctx {
 
     unsigned long long* claim;  // per triangle: (stamp<<32) | ~key
     int2* cand;                 // per queue entry: (4t+i, 4n+j) or (-1,-1)
-    int4* fmap;                 // per flipped triangle: old slot -> new (4t+s), .w = sub-round of the flip
     int* qst;                   // per triangle: queue stamp (dedup)
     int* queue;                 // flip queue (read)
     int* queue_next;            // flip queue (append)
@@ -176,16 +178,19 @@ GCDT_HD void setc(int4& v, int i, int x) {
     if (i == 0) v.x = x; else if (i == 1) v.y = x; else v.z = x;
 }
 GCDT_HD int slot_of(const int4& tv, int v) { return tv.x == v ? 0 : (tv.y == v ? 1 : 2); }
+GCDT_HD int slot_of_or_none(const int4& tv, int v) { return tv.x == v ? 0 : (tv.y == v ? 1 : (tv.z == v ? 2 : -1)); }
+// The flip sub-round kept in a vertex row's spare bits (see the layout).
+GCDT_HD int flip_stamp(int w) { return (int)((unsigned)w >> 4); }
 
 // A host test build may count triangle-record accesses by defining
 // GCDT_TOUCH; the library defines nothing here.
 #ifndef GCDT_TOUCH
-#define GCDT_TOUCH()
+#define GCDT_TOUCH(t)
 #endif
 
 // Vertex row (TV) and adjacency row (TA) of triangle t.
-GCDT_HD int4& tri_v(const Ctx& c, int t) { GCDT_TOUCH(); return c.tri[2 * (size_t)(unsigned)t]; }
-GCDT_HD int4& tri_a(const Ctx& c, int t) { GCDT_TOUCH(); return c.tri[2 * (size_t)(unsigned)t + 1]; }
+GCDT_HD int4& tri_v(const Ctx& c, int t) { GCDT_TOUCH(t); return c.tri[2 * (size_t)(unsigned)t]; }
+GCDT_HD int4& tri_a(const Ctx& c, int t) { GCDT_TOUCH(t); return c.tri[2 * (size_t)(unsigned)t + 1]; }
 
 GCDT_HD uint32_t hash32(uint32_t x) {  // bijective 32-bit mix
     x ^= x >> 16; x *= 0x7feb352dU;
@@ -354,7 +359,6 @@ GCDT_HD void body_clear(const Ctx& c, int t) {
     c.vote[t] = 0;
     c.claim[t] = 0;
     c.ins[t] = make_int2(0, 0);
-    c.fmap[t] = make_int4(-1, -1, -1, -1);
     c.qst[t] = 0;
 }
 
@@ -805,15 +809,40 @@ GCDT_HD void do_flip(const Ctx& c, int t, int i, int n, int j,
     int i1 = nx3(i), i2 = nx3(i1), j1 = nx3(j), j2 = nx3(j1);
     int A = comp(tv, i), B = comp(tv, i1), C = comp(tv, i2), D = comp(nv, j);
     int ft = tv.w, fn = nv.w;
-    tri_v(c, t) = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2));
+    // t keeps side 0 of the flip, n side 1; both carry the sub-round
+    const int stamp = (int)c.sr << 4;
+    tri_v(c, t) = make_int4(A, B, D, ((fn >> j1) & 1) | (((ft >> i2) & 1) << 2) | stamp);
     tri_a(c, t) = make_int4(comp(na, j1), enc(n, 2), comp(ta, i2), (int)c.round);
-    tri_v(c, n) = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1));
+    tri_v(c, n) = make_int4(A, D, C, ((fn >> j2) & 1) | (((ft >> i1) & 1) << 1) | 8 | stamp);
     tri_a(c, n) = make_int4(comp(na, j2), comp(ta, i1), enc(t, 1), (int)c.round);
-    int4 mt = make_int4(-1, -1, -1, (int)c.sr), mn = make_int4(-1, -1, -1, (int)c.sr);
-    setc(mt, i1, enc(n, 1)); setc(mt, i2, enc(t, 2));
-    setc(mn, j1, enc(t, 0)); setc(mn, j2, enc(n, 0));
-    c.fmap[t] = mt;
-    c.fmap[n] = mn;
+}
+
+// The edge in slot s of flipped triangle tt (vertex row tv) had the old
+// neighbour `old`; mv is that neighbour's vertex row now and mp its partner
+// slots (adjacency slots 1 and 2).  If that neighbour flipped in this
+// sub-round too, returns the triangle and slot that now hold the edge: its
+// own new triangle when both endpoints are in it, else its partner's --
+// the pair (A,B,D) side 0 / (A,D,C) side 1 has the outer edges BD, AB and
+// DC, CA, so the partner's slot follows from whether the edge ends at D.
+// Otherwise -1 (the old neighbour keeps the edge).  The partner slots are
+// the flip's new diagonal, which no fix pass writes.
+GCDT_HD int moved_edge(const Ctx& c, const int4& tv, int s, int old, const int4& mv, int2 mp) {
+    if (flip_stamp(mv.w) != (int)c.sr) return -1;
+    const int u = comp(tv, nx3(s)), v = comp(tv, nx3(nx3(s)));
+    const int su = slot_of_or_none(mv, u), sv = slot_of_or_none(mv, v);
+    if (su >= 0 && sv >= 0) return enc(old >> 2, 3 - su - sv);
+    if (((mv.w >> 3) & 1) == 0) {           // it became (A,B,D): the edge is DC or CA of (A,D,C)
+        const int D = mv.z;
+        return enc(mp.x >> 2, (u == D || v == D) ? 0 : 1);
+    }
+    const int D = mv.y;                      // it became (A,D,C): the edge is BD or AB of (A,B,D)
+    return enc(mp.y >> 2, (u == D || v == D) ? 0 : 2);
+}
+
+// The partner slots (adjacency slots 1 and 2) of triangle m.
+GCDT_HD int2 partner_slots(const Ctx& c, int m) {
+    const int* a = reinterpret_cast<const int*>(&tri_a(c, m));
+    return make_int2(a[1], a[2]);
 }
 
 GCDT_HD void body_flip_do(const Ctx& c, int k) {
@@ -868,12 +897,9 @@ GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
     int old = comp(*row, s);
     if (old < 0) return;
     int m = old >> 2, ms = old & 3;
-    int4 fm = c.fmap[m];
-    if (fm.w == (int)c.sr) {
-        ((int*)row)[s] = comp(fm, ms);
-    } else {
-        ((int*)&tri_a(c, m))[ms] = enc(tt, s);
-    }
+    const int e = moved_edge(c, tri_v(c, tt), s, old, tri_v(c, m), partner_slots(c, m));
+    if (e >= 0) ((int*)row)[s] = e;
+    else ((int*)&tri_a(c, m))[ms] = enc(tt, s);
 }
 
 // k < c.list_n: resolve the outer adjacency of flipped pair k.
@@ -883,7 +909,7 @@ GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
 GCDT_HD void body_flip_fix(const Ctx& c, int k) {
     if (k >= c.list_n) {
         int2 cd = c.cand[k - c.list_n];
-        if (cd.x >= 0 && c.fmap[cd.x >> 2].w != (int)c.sr)
+        if (cd.x >= 0 && flip_stamp(tri_v(c, cd.x >> 2).w) != (int)c.sr)
             c.queue_next[2 * c.list_n + append_slot(&c.cnt->cur_q, c.base_q)] = c.queue[k - c.list_n];
         return;
     }
@@ -895,13 +921,14 @@ GCDT_HD void body_flip_fix(const Ctx& c, int k) {
     resolve_flip_edge(c, n, 1);
 }
 
-// The edge in slot s of flipped triangle tt named the old neighbour `old`
-// (fm = fmap of that neighbour): the write resolve_flip_edge would make.
-GCDT_HD void resolve_flip_loaded(const Ctx& c, int tt, int s, int old, const int4& fm) {
+// The edge in slot s of flipped triangle tt (vertex row tv) named the old
+// neighbour `old` (mv, mp: its vertex row and partner slots now): the write
+// resolve_flip_edge would make.
+GCDT_HD void resolve_flip_loaded(const Ctx& c, int tt, const int4& tv, int s, int old, const int4& mv, int2 mp) {
     if (old < 0) return;
-    int m = old >> 2, ms = old & 3;
-    if (fm.w == (int)c.sr) ((int*)&tri_a(c, tt))[s] = comp(fm, ms);
-    else ((int*)&tri_a(c, m))[ms] = enc(tt, s);
+    const int e = moved_edge(c, tv, s, old, mv, mp);
+    if (e >= 0) ((int*)&tri_a(c, tt))[s] = e;
+    else ((int*)&tri_a(c, old >> 2))[old & 3] = enc(tt, s);
 }
 
 // Two items per thread (k1 < 0: only k0), as body_flip_fix on each, with
@@ -917,45 +944,58 @@ GCDT_HD void body_flip_fix_pair(const Ctx& c, int k0, int k1) {
         cd[u] = kind[u] == 2 ? c.cand[ks[u] - c.list_n] : make_int2(-1, -1);
         t[u] = kind[u] == 1 ? qtri(c.queue_next[2 * ks[u]]) : 0;
     }
-    int4 ta[2], fl[2];
+    int4 tv[2], ta[2];
+    int flw[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
+        tv[u] = kind[u] == 1 ? tri_v(c, t[u]) : none;
         ta[u] = kind[u] == 1 ? tri_a(c, t[u]) : none;
-        fl[u] = (kind[u] == 2 && cd[u].x >= 0) ? c.fmap[cd[u].x >> 2] : none;
+        flw[u] = (kind[u] == 2 && cd[u].x >= 0) ? tri_v(c, cd[u].x >> 2).w : 0;
     }
     // re-queue the candidates that did not flip and whose triangle nobody flipped
     int rq[2];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) rq[u] = (kind[u] == 2 && cd[u].x >= 0 && fl[u].w != (int)c.sr) ? 1 : 0;
+    for (int u = 0; u < 2; ++u) rq[u] = (kind[u] == 2 && cd[u].x >= 0 && flip_stamp(flw[u]) != (int)c.sr) ? 1 : 0;
     if (rq[0] | rq[1]) {
         int at = 2 * c.list_n + append_slots(&c.cnt->cur_q, c.base_q, rq[0] + rq[1]);
 #pragma unroll
         for (int u = 0; u < 2; ++u)
             if (rq[u]) c.queue_next[at++] = c.queue[ks[u] - c.list_n];
     }
-    // flipped pairs: t's outer edges 0, 2 and n's outer edges 0, 1
+    // flipped pairs: t's outer edges 0, 2 and n's outer edges 0, 1; each old
+    // neighbour's row (one sector, which the fix writes when that neighbour
+    // did not flip) tells whether it flipped and where the edge went
     int n[2];
-    int4 na[2], f0[2], f2[2];
+    int4 nv[2], na[2], m0[2], m2[2];
+    int2 p0[2], p2[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         n[u] = ta[u].y >> 2;
+        nv[u] = kind[u] == 1 ? tri_v(c, n[u]) : none;
         na[u] = kind[u] == 1 ? tri_a(c, n[u]) : none;
-        f0[u] = (kind[u] == 1 && ta[u].x >= 0) ? c.fmap[ta[u].x >> 2] : none;
-        f2[u] = (kind[u] == 1 && ta[u].z >= 0) ? c.fmap[ta[u].z >> 2] : none;
+        const bool l0 = kind[u] == 1 && ta[u].x >= 0, l2 = kind[u] == 1 && ta[u].z >= 0;
+        m0[u] = l0 ? tri_v(c, ta[u].x >> 2) : none;
+        p0[u] = l0 ? partner_slots(c, ta[u].x >> 2) : make_int2(-1, -1);
+        m2[u] = l2 ? tri_v(c, ta[u].z >> 2) : none;
+        p2[u] = l2 ? partner_slots(c, ta[u].z >> 2) : make_int2(-1, -1);
     }
     int4 g0[2], g1[2];
+    int2 q0[2], q1[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
-        g0[u] = (kind[u] == 1 && na[u].x >= 0) ? c.fmap[na[u].x >> 2] : none;
-        g1[u] = (kind[u] == 1 && na[u].y >= 0) ? c.fmap[na[u].y >> 2] : none;
+        const bool l0 = kind[u] == 1 && na[u].x >= 0, l1 = kind[u] == 1 && na[u].y >= 0;
+        g0[u] = l0 ? tri_v(c, na[u].x >> 2) : none;
+        q0[u] = l0 ? partner_slots(c, na[u].x >> 2) : make_int2(-1, -1);
+        g1[u] = l1 ? tri_v(c, na[u].y >> 2) : none;
+        q1[u] = l1 ? partner_slots(c, na[u].y >> 2) : make_int2(-1, -1);
     }
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         if (kind[u] != 1) continue;
-        resolve_flip_loaded(c, t[u], 0, ta[u].x, f0[u]);
-        resolve_flip_loaded(c, t[u], 2, ta[u].z, f2[u]);
-        resolve_flip_loaded(c, n[u], 0, na[u].x, g0[u]);
-        resolve_flip_loaded(c, n[u], 1, na[u].y, g1[u]);
+        resolve_flip_loaded(c, t[u], tv[u], 0, ta[u].x, m0[u], p0[u]);
+        resolve_flip_loaded(c, t[u], tv[u], 2, ta[u].z, m2[u], p2[u]);
+        resolve_flip_loaded(c, n[u], nv[u], 0, na[u].x, g0[u], q0[u]);
+        resolve_flip_loaded(c, n[u], nv[u], 1, na[u].y, g1[u], q1[u]);
     }
 }
 

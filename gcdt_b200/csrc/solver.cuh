@@ -76,7 +76,6 @@ __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     c.winners = (int2*)(base + p.o_win);
     c.claim = (unsigned long long*)(base + p.o_claim);
     c.cand = (int2*)(base + p.o_cand);
-    c.fmap = (int4*)(base + p.o_fmap);
     c.qst = (int*)(base + p.o_qst);
     c.queue = (int*)(base + p.o_qA);
     c.queue_next = (int*)(base + p.o_qB);
@@ -379,7 +378,6 @@ void enqueue_solve(BK& bk, Ctx c) {
     bk.fill(c.vote, 0, 8 * T);
     bk.fill(c.claim, 0, 8 * T);
     bk.fill(c.ins, 0, 8 * T);
-    bk.fill(c.fmap, 0xff, 16 * T);
     bk.fill(c.qst, 0, 4 * T);
     if (n > 0) {
         bk.launch(K_KEYS, c, n);

@@ -14,20 +14,28 @@
 #include <vector>
 #pragma nv_diag_suppress 20011
 #pragma nv_diag_suppress 20014
-// Triangle-record accesses (vertex row or adjacency row, read or write) per
-// phase kind, counted by the host runs of the bodies.
+// Triangle records (the 32-byte vertex + adjacency row pair, read or
+// written) touched per phase kind, counted once per item (per body call:
+// an item that reads a record and writes it back touches one sector), by
+// the host runs of the bodies.
 long long gcdt_host_touch[64];
 long long gcdt_host_items[64];
 // Flip-queue outcomes: entries checked, entries with a candidate edge,
 // distinct candidate edges, flips.
 long long g_fq[4];
 int gcdt_host_phase = 63;
-__host__ __device__ inline void gcdt_host_touch_one() {
+static int g_item_tris[64];
+static int g_item_n = 0;
+__host__ __device__ inline void gcdt_host_touch_one(int t) {
 #ifndef __CUDA_ARCH__
+    for (int k = 0; k < g_item_n; ++k)
+        if (g_item_tris[k] == t) return;
+    if (g_item_n < 64) g_item_tris[g_item_n++] = t;
     ++gcdt_host_touch[gcdt_host_phase];
 #endif
 }
-#define GCDT_TOUCH() gcdt_host_touch_one()
+inline void gcdt_host_new_item() { g_item_n = 0; }
+#define GCDT_TOUCH(t) gcdt_host_touch_one(t)
 #include "../gcdt_b200/csrc/solver.cuh"
 
 using namespace gcdt;
@@ -70,6 +78,7 @@ void host_phase(int k, const Ctx& c, long long n) {
         for (size_t m = 0; m < idx.size(); m += w) {
             int ks[4];
             for (size_t u = 0; u < 4; ++u) ks[u] = m + u < idx.size() && u < w ? idx[m + u] : -1;
+            gcdt_host_new_item();
             if (k == K_FLIP_CHECK && w == 2) body_flip_check_pair(c, ks[0], ks[1]);
             else if (k == K_FLIP_CHECK && w == 3) { const int k3[3] = {ks[0], ks[1], ks[2]}; flip_check_multi<3>(c, k3); }
             else if (k == K_FLIP_CHECK) { const int k4[4] = {ks[0], ks[1], ks[2], ks[3]}; flip_check_multi<4>(c, k4); }
@@ -77,9 +86,13 @@ void host_phase(int k, const Ctx& c, long long n) {
             else body_flip_fix_pair(c, ks[0], ks[1]);
         }
     } else {
-        for (int i : idx) dispatch(k, c, i);
+        for (int i : idx) {
+            gcdt_host_new_item();
+            dispatch(k, c, i);
+        }
     }
     gcdt_host_phase = 63;
+    gcdt_host_new_item();
     if (k == K_FLIP_CHECK) {
         std::vector<long long> edges;
         for (long long i = 0; i < n; ++i) {
