@@ -25,6 +25,22 @@ namespace gcdt {
 constexpr int kPersistBlock = GCDT_PERSIST_BLOCK;   // 512: one block per SM (128 registers per thread)
 constexpr int kPersistMinBlocks = GCDT_PERSIST_MINB;
 
+// The context a phase's items see: the launch's context `param` (in kernel
+// parameter space) with the fields the driver changes between phases taken
+// from the driver's copy `c`.  The other fields (the array pointers and
+// sizes) stay reads of parameter space, so the item loops keep them in no
+// register.
+__device__ __forceinline__ Ctx phase_view(const Ctx& param, const Ctx& c) {
+    Ctx v = param;
+    v.round = c.round; v.sr = c.sr; v.eslot = c.eslot; v.lawson_sr = c.lawson_sr;
+    v.list_n = c.list_n; v.carry_n = c.carry_n; v.level = c.level;
+    v.act = c.act; v.act_next = c.act_next; v.queue = c.queue; v.queue_next = c.queue_next;
+    v.pend = c.pend; v.pend_next = c.pend_next; v.lq = c.lq;
+    v.base_act = c.base_act; v.base_win = c.base_win; v.base_q = c.base_q; v.base_flip = c.base_flip;
+    v.base_pend = c.base_pend; v.base_law = c.base_law; v.base_scr = c.base_scr;
+    return v;
+}
+
 struct GridExec {
     static constexpr bool kCanNarrow = true;
     Counters* cnt;
@@ -40,6 +56,7 @@ struct GridExec {
     unsigned long long* snap;                // shared memory, kSnapWords entries
     unsigned spin_limit = 1u << 24;          // polls before a barrier wait gives up
     int* work = nullptr;                     // shared memory: the block's next item (dynamic phases)
+    const Ctx* param = nullptr;              // the launch's context, in kernel parameter space
 
     __device__ void take_snapshot() {
         volatile unsigned long long* src = reinterpret_cast<volatile unsigned long long*>(cnt);
@@ -92,7 +109,8 @@ struct GridExec {
         }
         __syncthreads();
     }
-    __device__ void phase(int k, const Ctx& c, long long count) {
+    __device__ void phase(int k, const Ctx& cd, long long count) {
+        const Ctx c = phase_view(*param, cd);
         const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
         long long t0 = threadIdx.x == 0 ? clock64() : 0;
         // the rounds' and flip sub-rounds' phases take their items in warp

@@ -38,11 +38,12 @@ __global__ void gcdt_predicates(const int2* q, int n, int* out) {
 
 static_assert(offsetof(Counters, cur_scr) + 8 <= GridExec::kSnapWords * 8, "cursors are in the snapshot");
 
-__global__ void __launch_bounds__(kPersistBlock, kPersistMinBlocks) gcdt_stages(Ctx c) {
+__global__ void __launch_bounds__(kPersistBlock, kPersistMinBlocks) gcdt_stages(const __grid_constant__ Ctx c) {
     __shared__ unsigned long long snap[GridExec::kSnapWords];
     __shared__ int work;
     GridExec ex{c.cnt, gridDim.x, snap};
     ex.work = &work;
+    ex.param = &c;
     if (threadIdx.x == 0) ex.take_snapshot();
     __syncthreads();
     run_stages(ex, c);
