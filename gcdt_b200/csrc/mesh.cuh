@@ -89,6 +89,9 @@ struct Counters {
     unsigned long long wcur_sum[2];
 };
 
+// The persistent kernel's phases see the launch's context with the fields
+// the stage driver changes between phases copied in (phase_view in
+// exec.cuh): a field the driver starts to change goes into that list.
 struct Ctx {
     int n;          // input points
     int s;          // input segments
@@ -299,20 +302,25 @@ GCDT_HD unsigned long long morton60(int2 p) {
 // the coordinates rotated into that quadrant's frame), a bijection onto
 // [0, 2^60) like the Morton code, with no jumps between quadrants.
 GCDT_HD unsigned long long hilbert60(int2 p) {
-    unsigned x = (unsigned)p.x & 0x3fffffffu, y = (unsigned)p.y & 0x3fffffffu;
+    // Level by level from the top bit, the quadrant of the point in the
+    // current sub-square gives two bits of the index; the sub-square's
+    // orientation is the transform that maps the raw coordinates onto its
+    // canonical frame: a swap of x and y (sw) composed with the complement
+    // of both (cp).  Both are involutions and commute, so two bits of state
+    // track it, updated without branches.  The index is the usual one:
+    // quadrant digit (3*rx) ^ ry, and a lower quadrant (ry = 0) swaps the
+    // frame, complemented first when rx = 1.
+    const unsigned x = (unsigned)p.x & 0x3fffffffu, y = (unsigned)p.y & 0x3fffffffu;
+    unsigned sw = 0, cp = 0;
     unsigned long long d = 0;
-    for (unsigned s = 1u << 29; s > 0; s >>= 1) {
-        const unsigned rx = (x & s) ? 1u : 0u, ry = (y & s) ? 1u : 0u;
-        d += (unsigned long long)s * s * ((3u * rx) ^ ry);
-        if (ry == 0) {
-            if (rx == 1) {
-                x = (s - 1) - (x & (s - 1));
-                y = (s - 1) - (y & (s - 1));
-            }
-            const unsigned t = x;
-            x = y;
-            y = t;
-        }
+#pragma unroll
+    for (int i = 29; i >= 0; --i) {
+        const unsigned a = ((x >> i) & 1u) ^ cp, b = ((y >> i) & 1u) ^ cp;
+        const unsigned rx = sw ? b : a, ry = sw ? a : b;
+        d = (d << 2) | ((3u * rx) ^ ry);
+        const unsigned lower = ry ^ 1u;
+        sw ^= lower;
+        cp ^= lower & rx;
     }
     return d;
 }

@@ -248,3 +248,9 @@ extern "C" void host_touch_counts(long long* out, long long* items) {
 extern "C" void host_flip_outcomes(long long* out) {
     for (int k = 0; k < 4; ++k) { out[k] = g_fq[k]; g_fq[k] = 0; }
 }
+
+// The sort keys of n points (2n int32 coordinates), as the key kernel
+// computes them.
+extern "C" void host_sort_keys(const int* xy, int n, unsigned long long* out) {
+    for (int i = 0; i < n; ++i) out[i] = gcdt::sort_key60(make_int2(xy[2 * i], xy[2 * i + 1]));
+}

@@ -156,3 +156,42 @@ def test_record_accesses_per_point():
     assert fo["flips"] <= fo["distinct_candidates"] <= fo["with_candidate"] <= fo["entries"]
     flips = acc.get("flip_check", 0) + acc.get("flip_do", 0) + acc.get("flip_fix", 0)
     assert 0.5 < flips / total < 0.75
+
+
+def _hilbert_index(x, y, n=1 << 30):
+    """Hilbert index of cell (x, y) of an n x n grid by the usual quadrant
+    rotation: the quadrant digit (3*rx) ^ ry per level from the top, and a
+    lower quadrant (ry = 0) reflects (when rx = 1) and transposes the rest."""
+    d, s = 0, n // 2
+    while s > 0:
+        rx, ry = int(x & s > 0), int(y & s > 0)
+        d += s * s * ((3 * rx) ^ ry)
+        if ry == 0:
+            if rx == 1:
+                x, y = n - 1 - x, n - 1 - y
+            x, y = y, x
+        s //= 2
+    return d
+
+
+def test_sort_keys_are_the_hilbert_index():
+    """The key the points are sorted by equals the Hilbert index of the
+    point's 30-bit coordinates, and in a 64 x 64 corner consecutive keys are
+    neighbouring cells (the curve's defining property)."""
+    L = ctypes.CDLL(build_host_emulation())
+    L.host_sort_keys.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    rng = np.random.default_rng(3)
+    xy = np.concatenate([rng.integers(0, 1 << 30, (3000, 2)),
+                         rng.integers(0, 64, (200, 2)),
+                         [[0, 0], [(1 << 30) - 1, (1 << 30) - 1], [0, (1 << 30) - 1], [(1 << 30) - 1, 0]]]
+                        ).astype(np.int32)
+    keys = np.zeros(len(xy), np.uint64)
+    L.host_sort_keys(xy.ctypes.data, len(xy), keys.ctypes.data)
+    want = [_hilbert_index(int(x), int(y)) for x, y in xy]
+    assert keys.tolist() == want
+    g64 = np.array([(x, y) for x in range(64) for y in range(64)], np.int32)
+    k64 = np.zeros(len(g64), np.uint64)
+    L.host_sort_keys(g64.ctypes.data, len(g64), k64.ctypes.data)
+    path = g64[np.argsort(k64)]
+    assert sorted(k64.tolist()) == list(range(64 * 64))
+    assert (np.abs(np.diff(path, axis=0)).sum(axis=1) == 1).all()
