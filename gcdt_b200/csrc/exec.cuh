@@ -160,6 +160,32 @@ struct GridExec {
         if ((threadIdx.x & 31) == 0) j = atomicAdd(work, 1);
         return __shfl_sync(0xffffffffu, j, 0);
     }
+    // The flip passes' chunk loop: each lane's two items of the next chunk
+    // have their first word (queue entry or candidate) loaded while the
+    // current chunk runs.
+    template <int P>
+    __device__ void pipelined(const Ctx& c, long long count, int j) {
+        const int lane = threadIdx.x & 31;
+        long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
+        int k0 = base + lane < count ? (int)(base + lane) : -1;
+        int k1 = base + lane + 32 < count ? (int)(base + lane + 32) : -1;
+        int2 f0 = flip_first(c, P, k0), f1 = flip_first(c, P, k1);
+        while (base < count) {
+            j = take_chunk();
+            const long long nb = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
+            const int n0 = nb + lane < count ? (int)(nb + lane) : -1;
+            const int n1 = nb + lane + 32 < count ? (int)(nb + lane + 32) : -1;
+            const int2 g0 = flip_first(c, P, n0), g1 = flip_first(c, P, n1);
+            if (k0 >= 0) {
+                const int ks[2] = {k0, k1};
+                const int2 f[2] = {f0, f1};
+                if (P == FP_CHECK) flip_check_multi_f<2>(c, ks, f);
+                else if (P == FP_DO) body_flip_do_pair_f(c, ks, f);
+                else body_flip_fix_pair_f(c, ks, f);
+            }
+            base = nb; k0 = n0; k1 = n1; f0 = g0; f1 = g1;
+        }
+    }
     __device__ void dynamic_items(int k, const Ctx& c, long long count) {
         if (threadIdx.x == 0) *work = 0;
         __syncthreads();
@@ -167,21 +193,17 @@ struct GridExec {
         const long long chunk = pair ? 64 : 32;
         const int lane = threadIdx.x & 31;
         int j = take_chunk();
+        if (pair) {
+            if (k == K_FLIP_CHECK) pipelined<FP_CHECK>(c, count, j);
+            else if (k == K_FLIP_DO) pipelined<FP_DO>(c, count, j);
+            else pipelined<FP_FIX>(c, count, j);
+            return;
+        }
         for (;;) {
             const long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * chunk;
             if (base >= count) break;
             const long long i0 = base + lane;
-            if (i0 < count) {
-                if (pair) {
-                    const long long i1 = i0 + 32;
-                    const int k1 = i1 < count ? (int)i1 : -1;
-                    if (k == K_FLIP_CHECK) body_flip_check_pair(c, (int)i0, k1);
-                    else if (k == K_FLIP_DO) body_flip_do_pair(c, (int)i0, k1);
-                    else body_flip_fix_pair(c, (int)i0, k1);
-                } else {
-                    dispatch(k, c, (int)i0);
-                }
-            }
+            if (i0 < count) dispatch(k, c, (int)i0);
             j = take_chunk();
         }
     }

@@ -747,13 +747,13 @@ GCDT_HD void body_flip_check(const Ctx& c, int k) {
 // thread for this latency-bound pass.  Same result as body_flip_check on
 // each entry.
 template <int W>
-GCDT_HD void flip_check_multi(const Ctx& c, const int (&ks)[W]) {
+GCDT_HD void flip_check_multi_f(const Ctx& c, const int (&ks)[W], const int2 (&f)[W]) {
     bool on[W];
     int t[W], mask[W];
 #pragma unroll
     for (int u = 0; u < W; ++u) {
         on[u] = ks[u] >= 0;
-        int qe = on[u] ? c.queue[ks[u]] : 0;
+        int qe = on[u] ? f[u].x : 0;
         t[u] = qtri(qe);
         mask[u] = qe & 7;
     }
@@ -797,6 +797,25 @@ GCDT_HD void flip_check_multi(const Ctx& c, const int (&ks)[W]) {
         at_max64(&c.claim[n], ck);
         c.cand[ks[u]] = make_int2(key, en);
     }
+}
+
+// The first word item k of a flip pass loads (the check: its queue entry;
+// the flip: its candidate; the fix: a flipped pair's queue entry or a
+// candidate), so that a caller can issue it early.
+enum FlipPass : int { FP_CHECK, FP_DO, FP_FIX };
+GCDT_HD int2 flip_first(const Ctx& c, int pass, int k) {
+    if (k < 0) return make_int2(-1, -1);
+    if (pass == FP_CHECK) return make_int2(c.queue[k], 0);
+    if (pass == FP_DO) return c.cand[k];
+    return k >= c.list_n ? c.cand[k - c.list_n] : make_int2(c.queue_next[2 * k], 0);
+}
+
+template <int W>
+GCDT_HD void flip_check_multi(const Ctx& c, const int (&ks)[W]) {
+    int2 f[W];
+#pragma unroll
+    for (int u = 0; u < W; ++u) f[u] = flip_first(c, FP_CHECK, ks[u]);
+    flip_check_multi_f<W>(c, ks, f);
 }
 
 GCDT_HD void body_flip_check_pair(const Ctx& c, int k0, int k1) {
@@ -873,11 +892,10 @@ GCDT_HD void body_flip_do(const Ctx& c, int k) {
 // Two candidates per thread (k1 < 0: only k0): the candidate and claim
 // loads of both are in flight together; the winners (a minority) then
 // flip one at a time, so only one pair of rows is live at once.
-GCDT_HD void body_flip_do_pair(const Ctx& c, int k0, int k1) {
-    const int ks[2] = {k0, k1};
+GCDT_HD void body_flip_do_pair_f(const Ctx& c, const int (&ks)[2], const int2 (&first)[2]) {
     int2 cd[2];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) cd[u] = ks[u] >= 0 ? c.cand[ks[u]] : make_int2(-1, -1);
+    for (int u = 0; u < 2; ++u) cd[u] = ks[u] >= 0 ? first[u] : make_int2(-1, -1);
     bool win[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
@@ -898,6 +916,12 @@ GCDT_HD void body_flip_do_pair(const Ctx& c, int k0, int k1) {
         qn[0] = qentry(t, 5);
         qn[1] = qentry(n, 3);
     }
+}
+
+GCDT_HD void body_flip_do_pair(const Ctx& c, int k0, int k1) {
+    const int ks[2] = {k0, k1};
+    const int2 f[2] = {flip_first(c, FP_DO, k0), flip_first(c, FP_DO, k1)};
+    body_flip_do_pair_f(c, ks, f);
 }
 
 GCDT_HD void resolve_flip_edge(const Ctx& c, int tt, int s) {
@@ -941,16 +965,15 @@ GCDT_HD void resolve_flip_loaded(const Ctx& c, int tt, const int4& tv, int s, in
 
 // Two items per thread (k1 < 0: only k0), as body_flip_fix on each, with
 // every stage's loads issued for both items first.
-GCDT_HD void body_flip_fix_pair(const Ctx& c, int k0, int k1) {
-    const int ks[2] = {k0, k1};
+GCDT_HD void body_flip_fix_pair_f(const Ctx& c, const int (&ks)[2], const int2 (&f)[2]) {
     const int4 none = make_int4(-1, -1, -1, -1);
     int kind[2], t[2];          // kind 0: nothing, 1: flipped pair, 2: candidate of the queue
     int2 cd[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         kind[u] = ks[u] < 0 ? 0 : (ks[u] >= c.list_n ? 2 : 1);
-        cd[u] = kind[u] == 2 ? c.cand[ks[u] - c.list_n] : make_int2(-1, -1);
-        t[u] = kind[u] == 1 ? qtri(c.queue_next[2 * ks[u]]) : 0;
+        cd[u] = kind[u] == 2 ? f[u] : make_int2(-1, -1);
+        t[u] = kind[u] == 1 ? qtri(f[u].x) : 0;
     }
     int4 tv[2], ta[2];
     int flw[2];
@@ -1005,6 +1028,12 @@ GCDT_HD void body_flip_fix_pair(const Ctx& c, int k0, int k1) {
         resolve_flip_loaded(c, n[u], nv[u], 0, na[u].x, g0[u], q0[u]);
         resolve_flip_loaded(c, n[u], nv[u], 1, na[u].y, g1[u], q1[u]);
     }
+}
+
+GCDT_HD void body_flip_fix_pair(const Ctx& c, int k0, int k1) {
+    const int ks[2] = {k0, k1};
+    const int2 f[2] = {flip_first(c, FP_FIX, k0), flip_first(c, FP_FIX, k1)};
+    body_flip_fix_pair_f(c, ks, f);
 }
 
 // ---------------------------------------------------------------- constraints
