@@ -163,8 +163,58 @@ struct GridExec {
     // The flip passes' chunk loop: each lane's two items of the next chunk
     // have their first word (queue entry or candidate) loaded while the
     // current chunk runs.
+#if defined(GCDT_PF2) || defined(GCDT_PFDO)
+    // L2 prefetch of the first row or claims item k of pass P loads after its
+    // first word f.
+    template <int P>
+    __device__ static void prefetch_first(const Ctx& c, int k, int2 f) {
+        if (k < 0) return;
+        const void* a = nullptr;
+        if (P == FP_CHECK) a = &c.tri[2 * (size_t)qtri(f.x)];
+        else if (P == FP_DO) { if (f.x >= 0) { a = &c.claim[f.x >> 2]; asm volatile("prefetch.global.L2 [%0];" :: "l"(&c.claim[f.y >> 2])); } }
+        else if (k < c.list_n) a = &c.tri[2 * (size_t)qtri(f.x)];
+        else if (f.x >= 0) a = &c.tri[2 * (size_t)(f.x >> 2)];
+        if (a) asm volatile("prefetch.global.L2 [%0];" :: "l"(a));
+    }
+    template <int P>
+    __device__ void pipelined2(const Ctx& c, long long count, int j) {
+        const int lane = threadIdx.x & 31;
+        long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
+        int k0 = base + lane < count ? (int)(base + lane) : -1;
+        int k1 = base + lane + 32 < count ? (int)(base + lane + 32) : -1;
+        int2 f0 = flip_first(c, P, k0), f1 = flip_first(c, P, k1);
+        j = take_chunk();
+        long long nb = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
+        int n0 = nb + lane < count ? (int)(nb + lane) : -1;
+        int n1 = nb + lane + 32 < count ? (int)(nb + lane + 32) : -1;
+        int2 g0 = flip_first(c, P, n0), g1 = flip_first(c, P, n1);
+        while (base < count) {
+            j = take_chunk();
+            const long long nnb = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
+            const int m0 = nnb + lane < count ? (int)(nnb + lane) : -1;
+            const int m1 = nnb + lane + 32 < count ? (int)(nnb + lane + 32) : -1;
+            const int2 h0 = flip_first(c, P, m0), h1 = flip_first(c, P, m1);
+            prefetch_first<P>(c, n0, g0);
+            prefetch_first<P>(c, n1, g1);
+            if (k0 >= 0) {
+                const int ks[2] = {k0, k1};
+                const int2 f[2] = {f0, f1};
+                if (P == FP_CHECK) flip_check_multi_f<2>(c, ks, f);
+                else if (P == FP_DO) body_flip_do_pair_f(c, ks, f);
+                else body_flip_fix_pair_f(c, ks, f);
+            }
+            base = nb; k0 = n0; k1 = n1; f0 = g0; f1 = g1;
+            nb = nnb; n0 = m0; n1 = m1; g0 = h0; g1 = h1;
+        }
+    }
+#endif
     template <int P>
     __device__ void pipelined(const Ctx& c, long long count, int j) {
+#if defined(GCDT_PF2)
+        pipelined2<P>(c, count, j); return;
+#elif defined(GCDT_PFDO)
+        if (P == FP_DO) { pipelined2<P>(c, count, j); return; }
+#endif
         const int lane = threadIdx.x & 31;
         long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
         int k0 = base + lane < count ? (int)(base + lane) : -1;
@@ -197,6 +247,45 @@ struct GridExec {
             if (k == K_FLIP_CHECK) pipelined<FP_CHECK>(c, count, j);
             else if (k == K_FLIP_DO) pipelined<FP_DO>(c, count, j);
             else pipelined<FP_FIX>(c, count, j);
+            return;
+        }
+        if (k == K_RELOC_VOTE || k == K_SPLIT) {
+            // two chunks ahead: the active points of chunk j+2 and the
+            // locations (and, for the relocation, coordinates) of chunk j+1's
+            // points are loaded while chunk j runs (each point's item is the
+            // only one that writes its location)
+            const bool rv = k == K_RELOC_VOTE;
+            long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * chunk;
+            int q = base + lane < count ? c.act[base + lane] : -1;
+            int t = q >= 0 ? c.loc[q] : -1;
+            int2 p = (rv && t >= 0) ? c.P[q] : make_int2(0, 0);
+            j = take_chunk();
+            long long nb = ((long long)blockIdx.x + (long long)j * gridDim.x) * chunk;
+            int nq = nb + lane < count ? c.act[nb + lane] : -1;
+            while (base < count) {
+                j = take_chunk();
+                const long long nnb = ((long long)blockIdx.x + (long long)j * gridDim.x) * chunk;
+                const int nnq = nnb + lane < count ? c.act[nnb + lane] : -1;
+                const int nt = nq >= 0 ? c.loc[nq] : -1;
+                const int2 np = (rv && nq >= 0) ? c.P[nq] : make_int2(0, 0);
+                if (q >= 0) {
+                    if (rv) body_reloc_vote_qt(c, q, t, p);
+                    else body_split_qt(c, q, t);
+                }
+                base = nb; q = nq; t = nt; p = np; nb = nnb; nq = nnq;
+            }
+            return;
+        }
+        if (k == K_FIX) {
+            long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * chunk;
+            int2 w = base + lane < count ? c.winners[base + lane] : make_int2(-1, -1);
+            while (base < count) {
+                j = take_chunk();
+                const long long nb = ((long long)blockIdx.x + (long long)j * gridDim.x) * chunk;
+                const int2 nw = nb + lane < count ? c.winners[nb + lane] : make_int2(-1, -1);
+                if (w.x >= 0) body_fix_f(c, w);
+                base = nb; w = nw;
+            }
             return;
         }
         for (;;) {

@@ -541,15 +541,13 @@ GCDT_HD int edge_of(const Ctx& c, int t, int2 p) {
     return o0 == 0 ? 0 : (o1 == 0 ? 1 : (o2 == 0 ? 2 : -1));
 }
 
-// Active point: relocate if its triangle changed in the previous round,
-// keep it in the next list, and vote for the triangle(s) it will split.
-// Winner per triangle = minimum hash32(q): random insertion order per
-// triangle, independent of thread scheduling.
-GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
-    int q = c.act[k];
-    int t = c.loc[q];
+// Active point q (its location t = loc[q] and coordinates p loaded by the
+// caller): relocate if its triangle changed in the previous round, keep it
+// in the next list, and vote for the triangle(s) it will split.  Winner per
+// triangle = minimum hash32(q): random insertion order per triangle,
+// independent of thread scheduling.
+GCDT_HD void body_reloc_vote_qt(const Ctx& c, int q, int t, int2 p) {
     if (t < 0) return;                       // inserted last round
-    int2 p = c.P[q];
     int e;
     if (tri_a(c, t).w == (int)c.round - 1) {
         int nt = walk(c, t, p, 256, &e);
@@ -571,6 +569,10 @@ GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
         int n = comp(tri_a(c, t), e) >> 2;
         if (c.vote[n] < key) at_max64(&c.vote[n], key);
     }
+}
+GCDT_HD void body_reloc_vote(const Ctx& c, int k) {
+    const int q = c.act[k], t = c.loc[q];
+    if (t >= 0) body_reloc_vote_qt(c, q, t, c.P[q]);
 }
 
 // Winners split their triangle(s).  Child j of a split triangle is the
@@ -631,12 +633,14 @@ GCDT_HD void split_winner(const Ctx& c, int q, int t, unsigned long long key) {
     c.winners[append_slot(&c.cnt->cur_win, c.base_win)] = make_int2(q, t);
 }
 
-GCDT_HD void body_split(const Ctx& c, int k) {
-    int q = c.act[k];
-    int t = c.loc[q];
+GCDT_HD void body_split_qt(const Ctx& c, int q, int t) {
     unsigned long long key = ((unsigned long long)c.round << 32) | (0xffffffffu - hash32((uint32_t)q));
     if (c.vote[t] != key) return;
     split_winner(c, q, t, key);
+}
+GCDT_HD void body_split(const Ctx& c, int k) {
+    const int q = c.act[k];
+    body_split_qt(c, q, c.loc[q]);
 }
 
 // Child of triangle m (split this round) that now holds m's old edge `ms`.
@@ -671,8 +675,7 @@ GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
 
 // Resolve outer adjacency of the children of one inserted point and queue
 // them for the flip phase (c.sr = first sub-round of this round).
-GCDT_HD void body_fix(const Ctx& c, int k) {
-    int2 w = c.winners[k];
+GCDT_HD void body_fix_f(const Ctx& c, int2 w) {
     int q = w.x, t = w.y;
     int T1 = 2 + 2 * q, T2 = 3 + 2 * q;
     int code = c.ins[t].y & 7;
@@ -702,6 +705,7 @@ GCDT_HD void body_fix(const Ctx& c, int k) {
         qn[2] = qentry(n, (1 << f1) | (1 << e2)); qn[3] = qentry(T2, (1 << f2) | (1 << e2));
     }
 }
+GCDT_HD void body_fix(const Ctx& c, int k) { body_fix_f(c, c.winners[k]); }
 
 // ---------------------------------------------------------------- flips
 
