@@ -163,58 +163,43 @@ struct GridExec {
     // The flip passes' chunk loop: each lane's two items of the next chunk
     // have their first word (queue entry or candidate) loaded while the
     // current chunk runs.
-#if defined(GCDT_PF2) || defined(GCDT_PFDO)
-    // L2 prefetch of the first row or claims item k of pass P loads after its
-    // first word f.
-    template <int P>
-    __device__ static void prefetch_first(const Ctx& c, int k, int2 f) {
-        if (k < 0) return;
-        const void* a = nullptr;
-        if (P == FP_CHECK) a = &c.tri[2 * (size_t)qtri(f.x)];
-        else if (P == FP_DO) { if (f.x >= 0) { a = &c.claim[f.x >> 2]; asm volatile("prefetch.global.L2 [%0];" :: "l"(&c.claim[f.y >> 2])); } }
-        else if (k < c.list_n) a = &c.tri[2 * (size_t)qtri(f.x)];
-        else if (f.x >= 0) a = &c.tri[2 * (size_t)(f.x >> 2)];
-        if (a) asm volatile("prefetch.global.L2 [%0];" :: "l"(a));
-    }
-    template <int P>
-    __device__ void pipelined2(const Ctx& c, long long count, int j) {
+    // The flip pass two chunks ahead: chunk j+2's candidates are loaded, and
+    // the claims chunk j+1's candidates name are prefetched into L2, while
+    // chunk j runs.  (The same second stage in the check and the fix, an L2
+    // prefetch of the rows their next chunk names, made them slower.)
+    __device__ void flip_do_pipelined(const Ctx& c, long long count, int j) {
         const int lane = threadIdx.x & 31;
-        long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
-        int k0 = base + lane < count ? (int)(base + lane) : -1;
-        int k1 = base + lane + 32 < count ? (int)(base + lane + 32) : -1;
-        int2 f0 = flip_first(c, P, k0), f1 = flip_first(c, P, k1);
+        auto chunk_at = [&](int jj) { return ((long long)blockIdx.x + (long long)jj * gridDim.x) * 64; };
+        auto item = [&](long long b, int o) { return b + lane + o < count ? (int)(b + lane + o) : -1; };
+        long long base = chunk_at(j);
+        int k0 = item(base, 0), k1 = item(base, 32);
+        int2 f0 = flip_first(c, FP_DO, k0), f1 = flip_first(c, FP_DO, k1);
         j = take_chunk();
-        long long nb = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
-        int n0 = nb + lane < count ? (int)(nb + lane) : -1;
-        int n1 = nb + lane + 32 < count ? (int)(nb + lane + 32) : -1;
-        int2 g0 = flip_first(c, P, n0), g1 = flip_first(c, P, n1);
+        long long nb = chunk_at(j);
+        int n0 = item(nb, 0), n1 = item(nb, 32);
+        int2 g0 = flip_first(c, FP_DO, n0), g1 = flip_first(c, FP_DO, n1);
         while (base < count) {
             j = take_chunk();
-            const long long nnb = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
-            const int m0 = nnb + lane < count ? (int)(nnb + lane) : -1;
-            const int m1 = nnb + lane + 32 < count ? (int)(nnb + lane + 32) : -1;
-            const int2 h0 = flip_first(c, P, m0), h1 = flip_first(c, P, m1);
-            prefetch_first<P>(c, n0, g0);
-            prefetch_first<P>(c, n1, g1);
+            const long long nnb = chunk_at(j);
+            const int m0 = item(nnb, 0), m1 = item(nnb, 32);
+            const int2 h0 = flip_first(c, FP_DO, m0), h1 = flip_first(c, FP_DO, m1);
+            if (n0 >= 0 && g0.x >= 0) prefetch_l2(&c.claim[g0.x >> 2], &c.claim[g0.y >> 2]);
+            if (n1 >= 0 && g1.x >= 0) prefetch_l2(&c.claim[g1.x >> 2], &c.claim[g1.y >> 2]);
             if (k0 >= 0) {
                 const int ks[2] = {k0, k1};
                 const int2 f[2] = {f0, f1};
-                if (P == FP_CHECK) flip_check_multi_f<2>(c, ks, f);
-                else if (P == FP_DO) body_flip_do_pair_f(c, ks, f);
-                else body_flip_fix_pair_f(c, ks, f);
+                body_flip_do_pair_f(c, ks, f);
             }
             base = nb; k0 = n0; k1 = n1; f0 = g0; f1 = g1;
             nb = nnb; n0 = m0; n1 = m1; g0 = h0; g1 = h1;
         }
     }
-#endif
+    __device__ static void prefetch_l2(const void* a, const void* b) {
+        asm volatile("prefetch.global.L2 [%0];" :: "l"(a));
+        asm volatile("prefetch.global.L2 [%0];" :: "l"(b));
+    }
     template <int P>
     __device__ void pipelined(const Ctx& c, long long count, int j) {
-#if defined(GCDT_PF2)
-        pipelined2<P>(c, count, j); return;
-#elif defined(GCDT_PFDO)
-        if (P == FP_DO) { pipelined2<P>(c, count, j); return; }
-#endif
         const int lane = threadIdx.x & 31;
         long long base = ((long long)blockIdx.x + (long long)j * gridDim.x) * 64;
         int k0 = base + lane < count ? (int)(base + lane) : -1;
@@ -245,7 +230,7 @@ struct GridExec {
         int j = take_chunk();
         if (pair) {
             if (k == K_FLIP_CHECK) pipelined<FP_CHECK>(c, count, j);
-            else if (k == K_FLIP_DO) pipelined<FP_DO>(c, count, j);
+            else if (k == K_FLIP_DO) flip_do_pipelined(c, count, j);
             else pipelined<FP_FIX>(c, count, j);
             return;
         }
@@ -319,11 +304,20 @@ struct GridExec {
 };
 
 // Executor of one block: a phase is a block-stride loop and a block barrier.
-// Used by block 0 for the short tails while the other blocks wait.
-struct BlockExec {
+// Used by block 0 for the short tails while the other blocks wait, and by
+// every block of the batched kernel (kView: the items see phase_view of
+// the block's context in shared memory).
+template <bool kView>
+struct BlockExecT {
     static constexpr bool kCanNarrow = false;
     Counters* cnt;
-    __device__ void phase(int k, const Ctx& c, long long count) {
+    const Ctx* base = nullptr;
+    __device__ void phase(int k, const Ctx& cd, long long count) {
+        if constexpr (kView) items(k, phase_view(*base, cd), count);
+        else items(k, cd, count);
+        __syncthreads();
+    }
+    __device__ void items(int k, const Ctx& c, long long count) {
         const long long stride = blockDim.x;
         long long i = threadIdx.x;
         // the latency-bound flip passes: two items per thread and trip, as
@@ -345,7 +339,6 @@ struct BlockExec {
         } else {
             for (; i < count; i += stride) dispatch(k, c, (int)i);
         }
-        __syncthreads();
     }
     __device__ unsigned long long cursor(unsigned long long* p) { return *(volatile unsigned long long*)p; }
     __device__ int word(int* p) { return *(volatile int*)p; }
@@ -360,6 +353,7 @@ struct BlockExec {
     __device__ int narrow_flips(Ctx&, Driver&, long long&) { return ST_INTERNAL; }
     __device__ int narrow_rounds(Ctx&, Driver&, long long) { return ST_INTERNAL; }
 };
+using BlockExec = BlockExecT<false>;
 
 static_assert(sizeof(Driver) <= sizeof(((Counters*)0)->handoff), "driver state fits the hand-off area");
 static_assert(sizeof(Driver) % 8 == 0, "driver state is whole 8-byte words");
