@@ -811,7 +811,8 @@ GCDT_HD int2 flip_first(const Ctx& c, int pass, int k) {
     if (k < 0) return make_int2(-1, -1);
     if (pass == FP_CHECK) return make_int2(c.queue[k], 0);
     if (pass == FP_DO) return c.cand[k];
-    return k >= c.list_n ? c.cand[k - c.list_n] : make_int2(c.queue_next[2 * k], 0);
+    // a flipped pair: both its queue entries (t's, then n's; 8-byte aligned)
+    return k >= c.list_n ? c.cand[k - c.list_n] : *reinterpret_cast<const int2*>(c.queue_next + 2 * k);
 }
 
 template <int W>
@@ -971,20 +972,25 @@ GCDT_HD void resolve_flip_loaded(const Ctx& c, int tt, const int4& tv, int s, in
 // every stage's loads issued for both items first.
 GCDT_HD void body_flip_fix_pair_f(const Ctx& c, const int (&ks)[2], const int2 (&f)[2]) {
     const int4 none = make_int4(-1, -1, -1, -1);
-    int kind[2], t[2];          // kind 0: nothing, 1: flipped pair, 2: candidate of the queue
+    int kind[2], t[2], n[2];    // kind 0: nothing, 1: flipped pair, 2: candidate of the queue
     int2 cd[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         kind[u] = ks[u] < 0 ? 0 : (ks[u] >= c.list_n ? 2 : 1);
         cd[u] = kind[u] == 2 ? f[u] : make_int2(-1, -1);
         t[u] = kind[u] == 1 ? qtri(f[u].x) : 0;
+        n[u] = kind[u] == 1 ? qtri(f[u].y) : 0;
     }
-    int4 tv[2], ta[2];
+    // both triangles of a flipped pair at once (the pair's two queue entries
+    // name them), so their old neighbours are one load further on
+    int4 tv[2], ta[2], nv[2], na[2];
     int flw[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
         tv[u] = kind[u] == 1 ? tri_v(c, t[u]) : none;
         ta[u] = kind[u] == 1 ? tri_a(c, t[u]) : none;
+        nv[u] = kind[u] == 1 ? tri_v(c, n[u]) : none;
+        na[u] = kind[u] == 1 ? tri_a(c, n[u]) : none;
         flw[u] = (kind[u] == 2 && cd[u].x >= 0) ? tri_v(c, cd[u].x >> 2).w : 0;
     }
     // re-queue the candidates that did not flip and whose triangle nobody flipped
@@ -1000,14 +1006,10 @@ GCDT_HD void body_flip_fix_pair_f(const Ctx& c, const int (&ks)[2], const int2 (
     // flipped pairs: t's outer edges 0, 2 and n's outer edges 0, 1; each old
     // neighbour's row (one sector, which the fix writes when that neighbour
     // did not flip) tells whether it flipped and where the edge went
-    int n[2];
-    int4 nv[2], na[2], m0[2], m2[2];
+    int4 m0[2], m2[2];
     int2 p0[2], p2[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
-        n[u] = ta[u].y >> 2;
-        nv[u] = kind[u] == 1 ? tri_v(c, n[u]) : none;
-        na[u] = kind[u] == 1 ? tri_a(c, n[u]) : none;
         const bool l0 = kind[u] == 1 && ta[u].x >= 0, l2 = kind[u] == 1 && ta[u].z >= 0;
         m0[u] = l0 ? tri_v(c, ta[u].x >> 2) : none;
         p0[u] = l0 ? partner_slots(c, ta[u].x >> 2) : make_int2(-1, -1);
