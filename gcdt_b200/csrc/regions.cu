@@ -7,9 +7,9 @@
 // across unconstrained edges), compress, seed, one expand pass per depth
 // level, depth.  Each pass reads the adjacency rows (12 B) and flags (1 B)
 // of its triangles in order plus the parent / level entries of neighbours,
-// which follow the mesh's Morton-coherent slot order; the expand rounds
-// number the greatest depth + 1 (2-3 for polygons with holes) and each costs
-// one 4-byte device-to-host read of its change flag.
+// which follow the mesh's slot order, coherent along the sort curve; the
+// expand rounds number the greatest depth + 1 (2-3 for polygons with holes)
+// and each costs one 4-byte device-to-host read of its change flag.
 #include <cuda_runtime.h>
 #include <climits>
 #include <cstdint>

@@ -122,7 +122,7 @@ gcdt_status gcdt_set_limits(gcdt_context* ctx, int32_t max_insertion_rounds,
    constrained Delaunay triangulation is unique under the fixed tie-break).
      levels          insertion levels, 1..4;
      level_stride    level k < levels-1 holds every level_stride[k]-th point
-                     of the Morton order not in a lower level (plus, for
+                     of the Hilbert order not in a lower level (plus, for
                      level 0, every segment endpoint); strictly decreasing,
                      >= 2; entries from levels-1 on are ignored;
      carry_queue     a round stops its flip sub-rounds once the queue is at
@@ -254,7 +254,7 @@ gcdt_status gcdt_classify_regions(const int32_t* d_adj, const uint8_t* d_cflags,
 
 /* ---- Batched triangulation (no counterpart in the reference, which
    triangulates one point set per process, kernel.cu:5332-5466).
-   Many independent instances in one launch: one segmented Morton sort,
+   Many independent instances in one launch: one segmented Hilbert sort,
    then one block per instance running the full solve, largest first.
    Instance i owns points [point_offsets[i], point_offsets[i+1]) of d_points
    and segments [segment_offsets[i], segment_offsets[i+1]) of d_segments,
