@@ -297,30 +297,58 @@ GCDT_HD unsigned long long morton60(int2 p) {
 // ---------------------------------------------------------------- set-up
 
 // One thread per input point: sort key + range check.
+// Four levels of the Hilbert index at a time: entry [frame][x bits << 4 |
+// y bits] holds the four quadrant digits (low 8 bits) and the frame after
+// them (bits 8-9).  Per level from the top bit, the quadrant of the point in
+// the current sub-square gives two bits of the index; the sub-square's frame
+// is the transform that maps the raw coordinates onto its canonical
+// orientation: a swap of x and y (bit 0) composed with the complement of
+// both (bit 1).  Both are involutions and commute, so the two bits track it.
+// The index is the usual one: quadrant digit (3*rx) ^ ry, and a lower
+// quadrant (ry = 0) swaps the frame, complemented first when rx = 1.
+struct HilbertTable { unsigned short v[4][256]; };
+__host__ __device__ constexpr HilbertTable make_hilbert_table() {
+    HilbertTable T{};
+    for (int frame = 0; frame < 4; ++frame)
+        for (int in = 0; in < 256; ++in) {
+            unsigned sw = frame & 1, cp = frame >> 1, d = 0;
+            for (int l = 3; l >= 0; --l) {
+                const unsigned a = ((in >> (4 + l)) & 1u) ^ cp, b = ((in >> l) & 1u) ^ cp;
+                const unsigned rx = sw ? b : a, ry = sw ? a : b;
+                d = (d << 2) | ((3u * rx) ^ ry);
+                const unsigned lower = ry ^ 1u;
+                sw ^= lower;
+                cp ^= lower & rx;
+            }
+            T.v[frame][in] = (unsigned short)(d | ((sw | (cp << 1)) << 8));
+        }
+    return T;
+}
+#if defined(__CUDACC__)
+__device__ constexpr HilbertTable kHilbertTableDev = make_hilbert_table();
+#endif
+constexpr HilbertTable kHilbertTable = make_hilbert_table();
+
 // Position of p along the Hilbert curve over the 2^30 x 2^30 grid (the
-// standard bit-by-bit construction: at each level the quadrant's index, then
-// the coordinates rotated into that quadrant's frame), a bijection onto
-// [0, 2^60) like the Morton code, with no jumps between quadrants.
+// standard construction: at each level the quadrant's index, then the
+// coordinates rotated into that quadrant's frame), a bijection onto
+// [0, 2^60) like the Morton code, with no jumps between quadrants.  The
+// coordinates are taken as 32-bit numbers: the two leading zero levels have
+// digit 0 and swap the frame twice, so the index is the 30-level one.
 GCDT_HD unsigned long long hilbert60(int2 p) {
-    // Level by level from the top bit, the quadrant of the point in the
-    // current sub-square gives two bits of the index; the sub-square's
-    // orientation is the transform that maps the raw coordinates onto its
-    // canonical frame: a swap of x and y (sw) composed with the complement
-    // of both (cp).  Both are involutions and commute, so two bits of state
-    // track it, updated without branches.  The index is the usual one:
-    // quadrant digit (3*rx) ^ ry, and a lower quadrant (ry = 0) swaps the
-    // frame, complemented first when rx = 1.
     const unsigned x = (unsigned)p.x & 0x3fffffffu, y = (unsigned)p.y & 0x3fffffffu;
-    unsigned sw = 0, cp = 0;
+    unsigned frame = 0;
     unsigned long long d = 0;
 #pragma unroll
-    for (int i = 29; i >= 0; --i) {
-        const unsigned a = ((x >> i) & 1u) ^ cp, b = ((y >> i) & 1u) ^ cp;
-        const unsigned rx = sw ? b : a, ry = sw ? a : b;
-        d = (d << 2) | ((3u * rx) ^ ry);
-        const unsigned lower = ry ^ 1u;
-        sw ^= lower;
-        cp ^= lower & rx;
+    for (int k = 28; k >= 0; k -= 4) {
+        const unsigned in = (((x >> k) & 15u) << 4) | ((y >> k) & 15u);
+#if defined(__CUDA_ARCH__)
+        const unsigned e = __ldg(&kHilbertTableDev.v[frame][in]);
+#else
+        const unsigned e = kHilbertTable.v[frame][in];
+#endif
+        d = (d << 8) | (e & 255u);
+        frame = e >> 8;
     }
     return d;
 }

@@ -4,6 +4,8 @@ The bar is bit-exact: the canonical triangle set (and the constraint flags
 rotated with it) must equal the oracle's, and the exact validator must pass
 on the GPU output (orientation, adjacency, hull, Euler count, constraints,
 local Delaunay under the shared tie-break)."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -136,3 +138,32 @@ def test_predicates_bit_equal_on_1e8_cases():
         assert len(bad) == 0, (bad[:5], q[bad[:5]].tolist(), dev[bad[:5]].tolist(), ref[bad[:5]].tolist())
         zeros += int((ref[:, 1] == 0).sum())
     assert zeros > 10_000_000
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,seed,args", [(g.GEN_SCALE, 5, (200000, 8, 40)), (g.GEN_LATTICE, 6, (256, 2000))],
+                         ids=["scale_200k", "lattice_256"])
+def test_gpu_bytes_equal_host_run_of_the_same_bodies(triangulator, kind, seed, args):
+    """The host run of the stage bodies (tests/host_emulation.cu) sorts the
+    points with the host copy of the key function and follows the GPU's
+    schedule; the output is independent of item order, so the device solve
+    must give the same bytes: triangles, adjacency and flags in the same
+    slots.  This pins the device's sort keys (a table in device memory) and
+    every device body to the host's."""
+    from tests.test_host_emulation import build_host_emulation
+    L = ctypes.CDLL(build_host_emulation())
+    vp, i32 = ctypes.c_void_p, ctypes.c_int
+    L.host_triangulate.argtypes = [vp, i32, vp, i32, vp, vp, vp, vp, i32, i32, i32]
+    L.host_triangulate.restype = i32
+    xy, cons = g.generate(kind, seed, *args)
+    xy = np.ascontiguousarray(xy, np.int32)
+    cons = np.ascontiguousarray(cons, np.int32).reshape(-1, 2)
+    T = 2 * len(xy) + 2
+    host = (np.zeros((T, 3), np.int32), np.zeros((T, 3), np.int32), np.zeros(T, np.uint8))
+    st = np.zeros(8, np.int64)
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)
+    rc = L.host_triangulate(p(xy), len(xy), p(cons), len(cons), p(host[0]), p(host[1]), p(host[2]), p(st), 0, 2, 0)
+    assert rc == 0
+    dev = triangulator.triangulate_host(xy, cons)
+    for a, b in zip(dev, host):
+        assert np.array_equal(a, b)
