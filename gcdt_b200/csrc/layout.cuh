@@ -26,7 +26,7 @@ struct Plan {
     size_t sort_temp_bytes;
     Layout L;
     size_t o_keys, o_keys_alt, o_vals, o_vals_alt, o_sort_tmp;
-    size_t o_P, o_perm, o_rank, o_tri, o_loc, o_pedge, o_actA, o_actB, o_vote, o_ins, o_win;
+    size_t o_P, o_perm, o_rank, o_tri, o_loc, o_pedge, o_actA, o_actB, o_vote, o_win;
     size_t o_claim, o_cand, o_qst, o_qA, o_qB;
     size_t o_seg, o_pendA, o_pendB, o_pinfo, o_scratch, o_vt, o_lvl, o_cnt;
 };
@@ -53,7 +53,6 @@ __host__ __device__ inline Plan make_plan(int64_t n, int64_t s, size_t sort_temp
     p.o_actA = L.take(4 * nn);
     p.o_actB = L.take(4 * nn);
     p.o_vote = L.take(8 * T);
-    p.o_ins = L.take(8 * T);
     p.o_win = L.take(8 * nn);
     p.o_claim = L.take(8 * T);
     p.o_cand = L.take(8 * T);

@@ -8,9 +8,10 @@
 //   perm[v]   int    input index of sorted point v (corners map to N+k)
 //   tri[2t]   int4   TV: (v0, v1, v2, w) -- CCW vertices; w bit k set when the
 //                    edge opposite v_k is a constraint edge (k < 3), bit 3 the
-//                    triangle's side of its last flip, bits 4.. the flip
-//                    sub-round of that flip (0: made by a split or a
-//                    constraint flip)
+//                    triangle's side of its last flip (or, after a split,
+//                    whether it was the second triangle of an edge split),
+//                    bits 4.. the flip sub-round of that flip (0: made by a
+//                    split or a constraint flip)
 //   tri[2t+1] int4   TA: (a0, a1, a2, -)  a_k = 4*n + j: neighbour n across the
 //                    edge opposite v_k, which is opposite slot j in n; -1 = box;
 //                    .w = the insertion round that last changed the triangle
@@ -122,7 +123,6 @@ struct Ctx {
     int* act;                 // active point list (read)
     int* act_next;            // active point list (append)
     unsigned long long* vote; // per triangle: (round<<32) | ~hash(point)
-    int2* ins;                // per triangle: (round, 8*q + split code)
     int2* winners;            // (q, t) inserted this round
 
     unsigned long long* claim;  // per triangle: (stamp<<32) | ~key
@@ -394,7 +394,6 @@ GCDT_HD void body_gather(const Ctx& c, int i) {
 GCDT_HD void body_clear(const Ctx& c, int t) {
     c.vote[t] = 0;
     c.claim[t] = 0;
-    c.ins[t] = make_int2(0, 0);
     c.qst[t] = 0;
 }
 
@@ -611,6 +610,7 @@ GCDT_HD void split_winner(const Ctx& c, int q, int t, unsigned long long key) {
     int T1 = 2 + 2 * q, T2 = 3 + 2 * q;
     int4 tv = tri_v(c, t), ta = tri_a(c, t);
     int fl = tv.w;
+    int code = e;
     if (e < 0) {
         int ch[3] = {t, T1, T2};
         for (int j = 0; j < 3; ++j) {
@@ -622,7 +622,7 @@ GCDT_HD void split_winner(const Ctx& c, int q, int t, unsigned long long key) {
             tri_v(c, ch[j]) = v;
             tri_a(c, ch[j]) = a;
         }
-        c.ins[t] = make_int2((int)c.round, q * 8 + 7);
+        code = 7;
     } else {
         int en = comp(ta, e);
         int n = en >> 2, e2 = en & 3;
@@ -644,8 +644,8 @@ GCDT_HD void split_winner(const Ctx& c, int q, int t, unsigned long long key) {
         a = make_int4(0, 0, 0, (int)c.round);
         setc(a, e_2, comp(ta, e_2)); setc(a, e1, enc(A1, e_2)); setc(a, e, enc(B1, e2));
         tri_v(c, A2) = v; tri_a(c, A2) = a;
-        // B1
-        v = nv; setc(v, f1, q); v.w = gl & ((1 << f1) | (1 << e2));
+        // B1 (bit 3: the second triangle of an edge split)
+        v = nv; setc(v, f1, q); v.w = (gl & ((1 << f1) | (1 << e2))) | 8;
         a = make_int4(0, 0, 0, (int)c.round);
         setc(a, f1, comp(na, f1)); setc(a, f2, enc(B2, f1)); setc(a, e2, enc(A2, e));
         tri_v(c, B1) = v; tri_a(c, B1) = a;
@@ -654,11 +654,9 @@ GCDT_HD void split_winner(const Ctx& c, int q, int t, unsigned long long key) {
         a = make_int4(0, 0, 0, (int)c.round);
         setc(a, f2, comp(na, f2)); setc(a, f1, enc(B1, f2)); setc(a, e2, enc(A1, e));
         tri_v(c, B2) = v; tri_a(c, B2) = a;
-        c.ins[t] = make_int2((int)c.round, q * 8 + e);
-        c.ins[n] = make_int2((int)c.round, q * 8 + 3 + e2);
     }
     c.loc[q] = -1;
-    c.winners[append_slot(&c.cnt->cur_win, c.base_win)] = make_int2(q, t);
+    c.winners[append_slot(&c.cnt->cur_win, c.base_win)] = make_int2(q * 8 + code, t);
 }
 
 GCDT_HD void body_split_qt(const Ctx& c, int q, int t) {
@@ -672,12 +670,23 @@ GCDT_HD void body_split(const Ctx& c, int k) {
 }
 
 // Child of triangle m (split this round) that now holds m's old edge `ms`.
-GCDT_HD int split_child(int2 im, int m, int ms) {
-    int code = im.y & 7, qm = im.y >> 3;
-    if (code == 7) return ms == 0 ? m : (ms == 1 ? 2 + 2 * qm : 3 + 2 * qm);
-    if (code < 3) return ms == nx3(code) ? m : 2 + 2 * qm;
-    int e = code - 3;
-    return ms == nx3(e) ? m : 3 + 2 * qm;
+// Triangle m was split this round too (its record mv is the child that kept
+// the slot m): the child of m that now holds the old edge in slot ms, whose
+// endpoints are the edge in slot s of triangle cv.  A child keeps the old
+// edge of the vertex it replaced; m's other children are 2+2q' and 3+2q'
+// for m's point q'.  A 1->3 split leaves q' in position 0 of m and edges 1,
+// 2 in 2+2q', 3+2q'; an edge split leaves q' where m's one outer edge it
+// keeps faces and its other outer edge in 2+2q' (first triangle) or 3+2q'
+// (second triangle, bit 3 of the flags).
+GCDT_HD int split_child(const int4& cv, int s, const int4& mv, int m, int ms) {
+    const int u = comp(cv, nx3(s)), v = comp(cv, nx3(nx3(s)));
+    const int p1 = nx3(ms), p2 = nx3(p1);
+    const int w1 = comp(mv, p1), w2 = comp(mv, p2);
+    const bool k1 = w1 == u || w1 == v, k2 = w2 == u || w2 == v;
+    if (k1 && k2) return m;
+    const int p = k1 ? p2 : p1;
+    const int qm = comp(mv, p);
+    return 2 + 2 * qm + (ms == nx3(p) ? ((mv.w >> 3) & 1) : 1);
 }
 
 // Flip-queue entry: triangle id << 3 | mask of the slots whose edges may
@@ -688,14 +697,19 @@ GCDT_HD int qtri(int e) { return (int)((unsigned)e >> 3); }
 // The children of the inserted points are distinct triangles, so the first
 // flip queue of a round needs no de-duplication.
 
+// The edge in slot s of split child ch names its old neighbour: point it at
+// the neighbour's child that holds the edge when the neighbour was split in
+// this round too (its adjacency row's round stamp; flips of the round come
+// after this phase), else write ch into the neighbour's row.  The
+// neighbour's record is the sector the second case writes anyway.
 GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
     int4* row = &tri_a(c, ch);
     int old = comp(*row, s);
     if (old < 0) return;
     int m = old >> 2, ms = old & 3;
-    int2 im = c.ins[m];
-    if (im.x == (int)c.round) {
-        ((int*)row)[s] = enc(split_child(im, m, ms), ms);
+    const int4 mv = tri_v(c, m), ma = tri_a(c, m);
+    if (ma.w == (int)c.round) {
+        ((int*)row)[s] = enc(split_child(tri_v(c, ch), s, mv, m, ms), ms);
     } else {
         ((int*)&tri_a(c, m))[ms] = enc(ch, s);
     }
@@ -704,9 +718,9 @@ GCDT_HD void resolve_split_edge(const Ctx& c, int ch, int s) {
 // Resolve outer adjacency of the children of one inserted point and queue
 // them for the flip phase (c.sr = first sub-round of this round).
 GCDT_HD void body_fix_f(const Ctx& c, int2 w) {
-    int q = w.x, t = w.y;
+    int q = w.x >> 3, t = w.y;
     int T1 = 2 + 2 * q, T2 = 3 + 2 * q;
-    int code = c.ins[t].y & 7;
+    int code = w.x & 7;
     // Only the old edges need a test: a spoke from q to a corner of the split
     // triangle is locally Delaunay (q lies inside the old empty circumcircle,
     // so the circle through q and the spoke's far edge excludes the third
@@ -745,10 +759,11 @@ GCDT_HD void body_fix(const Ctx& c, int k) { body_fix_f(c, c.winners[k]); }
 GCDT_HD void body_flip_check(const Ctx& c, int k) {
     int qe = c.queue[k];
     int t = qtri(qe), mask = qe & 7;
-    // a carried entry whose triangle was split this round: the split's own
-    // queue entries test every old edge of it
-    if (k < c.carry_n && c.ins[t].x == (int)c.round) { c.cand[k] = make_int2(-1, -1); return; }
     int4 tv = tri_v(c, t), ta = tri_a(c, t);
+    // a carried entry (first sub-round of a round, before its flips) whose
+    // triangle was split this round: the split's own queue entries test
+    // every old edge of it
+    if (k < c.carry_n && ta.w == (int)c.round) { c.cand[k] = make_int2(-1, -1); return; }
     // the edges to test: in the mask, with a neighbour, not constraints
     int live = mask & ~tv.w & ((ta.x >= 0) | ((ta.y >= 0) << 1) | ((ta.z >= 0) << 2));
     // issue every test's loads before the first test, so the neighbour rows
@@ -789,14 +804,17 @@ GCDT_HD void flip_check_multi_f(const Ctx& c, const int (&ks)[W], const int2 (&f
         t[u] = qtri(qe);
         mask[u] = qe & 7;
     }
-#pragma unroll
-    for (int u = 0; u < W; ++u)
-        if (on[u] && ks[u] < c.carry_n && c.ins[t[u]].x == (int)c.round) on[u] = false;
     int4 tv[W], ta[W];
 #pragma unroll
     for (int u = 0; u < W; ++u) {
         tv[u] = on[u] ? tri_v(c, t[u]) : make_int4(0, 0, 0, 7);
         ta[u] = on[u] ? tri_a(c, t[u]) : make_int4(-1, -1, -1, 0);
+        // a carried entry whose triangle was split this round (as above)
+        if (on[u] && ks[u] < c.carry_n && ta[u].w == (int)c.round) {
+            on[u] = false;
+            tv[u] = make_int4(0, 0, 0, 7);
+            ta[u] = make_int4(-1, -1, -1, 0);
+        }
     }
     int live[W], d[W][3];
 #pragma unroll

@@ -72,7 +72,6 @@ __host__ __device__ inline Ctx bind_ctx(char* base, const Plan& p) {
     c.act = (int*)(base + p.o_actA);
     c.act_next = (int*)(base + p.o_actB);
     c.vote = (unsigned long long*)(base + p.o_vote);
-    c.ins = (int2*)(base + p.o_ins);
     c.winners = (int2*)(base + p.o_win);
     c.claim = (unsigned long long*)(base + p.o_claim);
     c.cand = (int2*)(base + p.o_cand);
@@ -377,7 +376,6 @@ void enqueue_solve(BK& bk, Ctx c) {
     bk.fill(c.cnt, 0, sizeof(Counters));
     bk.fill(c.vote, 0, 8 * T);
     bk.fill(c.claim, 0, 8 * T);
-    bk.fill(c.ins, 0, 8 * T);
     bk.fill(c.qst, 0, 4 * T);
     if (n > 0) {
         bk.launch(K_KEYS, c, n);
