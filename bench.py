@@ -16,8 +16,8 @@ the one-step-at-a-time figure.
 
 At N = 1 the default run also reports, after the timed region: the exact
 validation of the timed output, the single-threaded CPU oracle on the same
-instance (`cpu_baseline`), the reference's own CUDA build on the same
-instance and on its own default input (`reference_cuda`), the degenerate
+instance (`cpu_baseline`), our time on the reference's own default input
+beside the reference CUDA build's recorded times (`reference_cuda`), the degenerate
 lattice workload (`lattice`), the 4,096-instance batched workload
 (`batched`) and the 20,000-request serving stream (`serving`).
 `--headline-only` skips them.
@@ -507,43 +507,43 @@ def _time_solves(tri, d_xy, d_cons, steps, warmup, dev, out=None):
     return statistics.median(ms), r
 
 
+REFERENCE_CUDA_FAULT = (
+    "not run: the reference's own CUDA build (oracle/_ref/gcdt_ref) raised cudaErrorIllegalAddress "
+    "(its include/utils.cuh:78, after its constraint stage) on the headline instance in one run on this "
+    "pool, so its GPU code is not run again; its figures below are the recorded ones")
+
+
 def measure_reference_cuda(args, xy, cons, dev):
-    """The reference's own CUDA pipeline (yingtix/gCDT built for sm_100a from
-    its sources, run as a separate process that replays its driver's stage
-    sequence, kernel.cu:5398-5443) on (i) the headline instance and (ii) its
-    own default input, 9M uniform points (kernel.cu:43-58), where its output
-    is complete; ours is timed on the same 9M input beside it.  The
-    reference's time is its outer cudaEvent pair around the stages, inputs
-    on the device."""
+    """The comparison with the reference's own CUDA pipeline (yingtix/gCDT
+    built for sm_100a from its sources, replaying its driver's stage
+    sequence, kernel.cu:5398-5443).  That build faulted on the headline
+    instance in one of its runs here, so it is not run: its times come from
+    the recorded fixtures (tests/golden/reference_fixtures.json, its outer
+    cudaEvent pair around the stages, inputs on the device), and ours is
+    timed live on the same 9M uniform input (its own default distribution,
+    kernel.cu:43-58), where its output is complete, with our triangle set
+    checked against the SHA-256 it recorded."""
+    import hashlib
     import torch
     import gcdt_b200 as g
-    from oracle import reference
-    if not reference.available():
-        return {"unavailable": "oracle/_ref/gcdt_ref not built (reference sources absent at build time)"}
-    os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")   # no lazy module loads inside its timed stages
-    res = {"kind": "reference CUDA build, one solve per process, stage timer = outer cudaEvent pair"}
-    r = reference.run(xy, cons, repeat=1, timeout=300)
-    res["headline"] = {
-        "ref_ms": r["event_ms"], "ref_sum_time_ms": r["sum_time"], "ref_triangles": int(len(r["tris"])),
-        "ref_ignored_segments": r["ignored"][-1] if r["ignored"] else None,
-        "ref_final_mark": r["marks"][-1] if r["marks"] else None,
-        "ours_ms": None, "n_points": len(xy), "n_segments": len(cons),
-        "ref_mpts_per_s": len(xy) / (r["event_ms"] * 1e-3) / 1e6}
-    uxy, _ = g.generate(g.GEN_UNIFORM, 13159, 9_000_000)
-    refs = [reference.run(uxy, None, repeat=1, timeout=300) for _ in range(2)]
+    with open(os.path.join(ROOT, "tests", "golden", "reference_fixtures.json")) as f:
+        cases = {c["name"]: c for c in json.load(f)["cases"]}
+    head, uni = cases["scale_10m_200k_segments"], cases["uniform_9m"]
+    res = {"kind": "reference CUDA build, recorded runs (tests/golden/reference_fixtures.json)",
+           "unavailable": REFERENCE_CUDA_FAULT}
+    res["headline"] = {"ref_ms_recorded": head["ref_event_ms"], "ref_ignored_segments": head["ref_ignored"],
+                       "n_points": head["n"], "n_segments": head["s"]}
+    uxy, _ = g.generate(g.GEN_UNIFORM, uni["seed"], *uni["args"])
     ours = g.Triangulator(max_points=len(uxy), max_segments=1, device=dev.index)
     d_u = torch.from_numpy(uxy).to(dev)
     ours_ms, (tris, _, _) = _time_solves(ours, d_u, None, max(5, args.steps // 2), 3, dev)
     ours_tris = tris.cpu().numpy()
     ours.close()
-    same = bool(np.array_equal(g.canonical(ours_tris), g.canonical(refs[-1]["tris"])))
-    ref_ms = statistics.median([x["event_ms"] for x in refs])
+    digest = hashlib.sha256(np.ascontiguousarray(g.canonical(ours_tris), dtype=np.int64).tobytes()).hexdigest()
     res["uniform_9m"] = {
-        "ref_ms": ref_ms, "ref_ms_runs": [x["event_ms"] for x in refs],
-        "ref_sum_time_ms": refs[-1]["sum_time"], "ref_final_mark": refs[-1]["marks"][-1] if refs[-1]["marks"] else None,
-        "ours_ms": ours_ms, "speedup": ref_ms / ours_ms, "identical_triangle_set": same,
-        "n_points": len(uxy), "ref_mpts_per_s": len(uxy) / (ref_ms * 1e-3) / 1e6,
-        "ours_mpts_per_s": len(uxy) / (ours_ms * 1e-3) / 1e6}
+        "ref_ms_recorded": uni["ref_event_ms"], "ours_ms": ours_ms, "speedup": uni["ref_event_ms"] / ours_ms,
+        "identical_to_recorded_reference_set": digest == uni["tris_sha256"],
+        "n_points": len(uxy), "ours_mpts_per_s": len(uxy) / (ours_ms * 1e-3) / 1e6}
     return res
 
 

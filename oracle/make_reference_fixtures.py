@@ -37,9 +37,14 @@ CASES = [
     ("uniform_1m", g.GEN_UNIFORM, 13159, [1000000], False),
     ("uniform_9m", g.GEN_UNIFORM, 13159, [9000000], False),
     ("scale_points_10m", g.GEN_SCALE, 1, [], True),
-    ("scale_10m_200k_segments", g.GEN_SCALE, 1, [], False),
     ("small_100k_512_segments", g.GEN_SMALL, 1, [], False),
 ]
+# The 10.2M-point + 200k-segment scale instance ("scale_10m_200k_segments",
+# GEN_SCALE seed 1 with its segments) is not re-run: the reference raised
+# cudaErrorIllegalAddress (its include/utils.cuh:78, after its constraint
+# stage) on it in one run, and reference GPU code that faulted is not run
+# again.  Its recorded entry is kept when the file is rewritten.
+KEEP_RECORDED = ("scale_10m_200k_segments",)
 
 
 def sha(a):
@@ -53,7 +58,7 @@ def main():
     out = {"reference": "yingtix/gCDT device pipeline, kernel.cu:5398-5443, built by oracle/build_ref.sh",
            "cases": []}
     old = {}
-    if only and os.path.exists(path):
+    if os.path.exists(path):
         with open(path) as f:
             old = {c["name"]: c for c in json.load(f)["cases"]}
     for name, kind, seed, args, drop in CASES:
@@ -77,6 +82,7 @@ def main():
                 "points_sha256": sha(r["points"])}
         out["cases"].append(case)
         print(json.dumps(case), flush=True)
+    out["cases"] += [old[name] for name in KEEP_RECORDED if name in old]
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", path)
