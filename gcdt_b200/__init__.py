@@ -103,6 +103,8 @@ def lib():
     L.gcdt_get_stats.restype = ctypes.c_int
     L.gcdt_status_string.argtypes = [ctypes.c_int]
     L.gcdt_status_string.restype = ctypes.c_char_p
+    L.gcdt_set_profiling.argtypes = [vp, i32]
+    L.gcdt_set_profiling.restype = ctypes.c_int
     L.gcdt_get_phase_profile.argtypes = [vp, vp, vp, i32]
     L.gcdt_get_phase_profile.restype = i32
     L.gcdt_get_phase_balance.argtypes = [vp, vp, vp, vp, i32]
@@ -304,6 +306,13 @@ class Triangulator:
         if rc != 0:
             raise GcdtError(rc, "gcdt_set_grid_blocks")
 
+    def set_profiling(self, on=True):
+        """Record the per-phase profile and balance of later solves
+        (gcdt_set_profiling; off by default: it costs a little time)."""
+        rc = lib().gcdt_set_profiling(self._h, 1 if on else 0)
+        if rc != 0:
+            raise GcdtError(rc, "gcdt_set_profiling")
+
     def triangulate_async(self, points, segments=None, out=None, stream=None):
         """Enqueue a solve on `stream` (default: the current stream) and return
         the output tensors at once; wait() reports the solve's status.  The
@@ -399,7 +408,8 @@ class Triangulator:
         return t.as_dict()
 
     def phase_profile(self):
-        """{phase name: (SM cycles, runs)} of the last solve's persistent kernel."""
+        """{phase name: (SM cycles, runs)} of the last solve's persistent
+        kernel; empty unless that solve ran with set_profiling(True)."""
         cyc = np.zeros(32, np.int64)
         cnt = np.zeros(32, np.int64)
         k = lib().gcdt_get_phase_profile(self._h, ctypes.c_void_p(cyc.ctypes.data),

@@ -38,12 +38,16 @@ __global__ void gcdt_predicates(const int2* q, int n, int* out) {
 
 static_assert(offsetof(Counters, cur_scr) + 8 <= GridExec::kSnapWords * 8, "cursors are in the snapshot");
 
+// kProf: the per-phase profile and balance are recorded (gcdt_set_profiling);
+// the instance without them carries none of their code.
+template <bool kProf>
 __global__ void __launch_bounds__(kPersistBlock, kPersistMinBlocks) gcdt_stages(const __grid_constant__ Ctx c) {
     __shared__ unsigned long long snap[GridExec::kSnapWords];
     __shared__ int work;
     GridExec ex{c.cnt, gridDim.x, snap};
     ex.work = &work;
     ex.param = &c;
+    ex.prof = kProf;
     if (threadIdx.x == 0) ex.take_snapshot();
     __syncthreads();
     run_stages(ex, c);
@@ -102,20 +106,22 @@ struct DeviceBackend {
     // All rounds run in one cooperative launch sized to the co-resident
     // block count, so every block is resident and the grid barrier is safe.
     int grid_limit = 0;   // at most this many blocks (0: no limit)
+    bool profile = false; // launch the stage kernel that records the phase profile
     cudaEvent_t ev_stage0 = nullptr, ev_stage1 = nullptr;   // recorded around the stage launch when set
     void stages(const Ctx& c) {
         if (err != cudaSuccess) return;
         int dev = 0, sms = 0, per_sm = 0;
         note(cudaGetDevice(&dev));
         note(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        note(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gcdt_stages, kPersistBlock, 0));
+        const void* kern = profile ? (const void*)gcdt_stages<true> : (const void*)gcdt_stages<false>;
+        note(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPersistBlock, 0));
         if (err != cudaSuccess || sms <= 0 || per_sm <= 0) { note(cudaErrorLaunchOutOfResources); return; }
         int blocks = sms * per_sm;
         if (grid_limit > 0 && grid_limit < blocks) blocks = grid_limit;
         Ctx cc = c;
         void* args[] = {&cc};
         if (ev_stage0) note(cudaEventRecord(ev_stage0, st));
-        note(cudaLaunchCooperativeKernel((const void*)gcdt_stages, dim3(blocks), dim3(kPersistBlock),
+        note(cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(kPersistBlock),
                                          args, 0, st));
         if (ev_stage1) note(cudaEventRecord(ev_stage1, st));
         launches++;
@@ -193,6 +199,8 @@ struct gcdt_context {
     gcdt_tuning tuning = default_tuning();
     // blocks of the persistent launch (0: all co-resident blocks)
     int32_t grid_blocks = 0;
+    // per-phase profiling of the stage kernel (gcdt_set_profiling)
+    int32_t profile = 0;
 };
 
 namespace {
@@ -286,6 +294,7 @@ gcdt_status enqueue(gcdt_context* ctx, const int32_t* d_points, int32_t n, const
     bk.sort_tmp = ctx->arena + plan.o_sort_tmp;
     bk.sort_bytes = plan.sort_temp_bytes;
     bk.grid_limit = ctx->grid_blocks;
+    bk.profile = ctx->profile != 0;
     bk.ev_stage0 = ctx->evs0;
     bk.ev_stage1 = ctx->evs1;
     bk.note(cudaEventRecord(ctx->evs0, bk.st));   // both stage events exist even if the launch is skipped
@@ -407,6 +416,12 @@ extern "C" gcdt_status gcdt_set_limits(gcdt_context* ctx, int32_t max_insertion_
     return GCDT_OK;
 }
 
+extern "C" gcdt_status gcdt_set_profiling(gcdt_context* ctx, int32_t on) {
+    if (!ctx) return GCDT_BAD_INPUT;
+    ctx->profile = on ? 1 : 0;
+    return GCDT_OK;
+}
+
 extern "C" gcdt_status gcdt_set_tuning(gcdt_context* ctx, const gcdt_tuning* tuning) {
     if (!ctx) return GCDT_BAD_INPUT;
     if (!tuning) { ctx->tuning = default_tuning(); return GCDT_OK; }
@@ -487,7 +502,7 @@ extern "C" gcdt_status gcdt_time_barriers(int device, int32_t rounds, double* us
     DeviceGuard g(device);
     int sms = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gcdt_stages, kPersistBlock, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gcdt_stages<false>, kPersistBlock, 0) != cudaSuccess ||
         sms <= 0 || per_sm <= 0) {
         cudaGetLastError();
         return GCDT_CUDA_ERROR;

@@ -69,8 +69,8 @@ struct Counters {
     unsigned long long cur_pend; // pending segment lists
     unsigned long long cur_law;  // constrained flip pass queue
     unsigned long long cur_scr;  // constraint scratch
-    unsigned int bar_count;      // grid barrier
-    unsigned int bar_gen;
+    unsigned int bar_count;      // grid barrier (top bit flips once per barrier)
+    unsigned int pad_bar;
     long long rounds, flip_subrounds, constraint_rounds;
     long long grid_blocks;       // blocks of the persistent launch
     long long pad1[2];

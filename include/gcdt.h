@@ -177,14 +177,22 @@ gcdt_status gcdt_probe_barrier(int device, int32_t blocks, int32_t absent_block,
    counterpart in the reference. */
 gcdt_status gcdt_time_barriers(int device, int32_t rounds, double* us_per_barrier);
 
-/* Per-phase profile of the last solve on ctx: SM cycles spent in each phase
+/* Per-phase profiling of ctx's later solves (no counterpart in the
+   reference): on (nonzero), the stage kernel records the two read-outs
+   below; off (the default), it records neither and their counters stay 0.
+   The records cost a few atomics and counter updates per phase (0.5% of
+   the 10M-point solve), so timed runs leave it off.  Returns GCDT_OK. */
+gcdt_status gcdt_set_profiling(gcdt_context* ctx, int32_t on);
+
+/* Per-phase profile of the last solve on ctx, if it ran with profiling on
+   (gcdt_set_profiling): SM cycles spent in each phase
    kind of the persistent stage kernel (measured by block 0, barrier wait
    included) and how often it ran.  Returns the number of phase kinds
    (names: gcdt_phase_name), or -1 on bad arguments.  Counters of the
    reference's per-stage cudaEvent printouts (e.g. rawMesh.cu:1008-1031). */
 int32_t gcdt_get_phase_profile(const gcdt_context* ctx, int64_t* cycles, int64_t* counts, int32_t max_kinds);
-/* Balance of the grid-wide phases of the last solve (no counterpart in the
-   reference): per phase kind, the sum over its runs of the longest block's
+/* Balance of the grid-wide phases of the last solve, if it ran with
+   profiling on (no counterpart in the reference): per phase kind, the sum over its runs of the longest block's
    work time (wmax) and of all blocks' work times (wsum), in SM cycles, the
    work time of a block being the time from the phase's start to its arrival
    at the phase's barrier.  wmax against the phase's cycles from
