@@ -49,9 +49,9 @@ UNIT = "Mpts/s"
 WORKLOAD = "plain CDT at scale: 10M Gaussian-mixture/uniform int32 points in [1,2^30-2]^2 + 3,125 star polygons (200,000 segments)"
 # DRAM bytes (read + write) of the stage kernel per point, from an ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum) of the same workload shape at
-# 1,020,608 points: 818,750,208 + 656,677,120 bytes.  Reported per solve as
+# 1,020,608 points: 799,542,272 + 648,609,536 bytes.  Reported per solve as
 # this figure times N (the full-size capture would replay a 2.4 GB arena ~40x).
-DRAM_BYTES_PER_POINT = (818750208 + 656677120) / 1020608
+DRAM_BYTES_PER_POINT = (799542272 + 648609536) / 1020608
 
 
 def rank_info():
