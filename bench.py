@@ -370,7 +370,15 @@ def run_ours(args):
         j = k & 1
         st_k = streams[j]
         if k == args.warmup:
-            # timed region: from here, both streams' later work comes after t_start
+            # timed region: it starts on an idle device, every warm-up step's
+            # solve and copies finished (recording it behind the warm-up work
+            # still in the streams would count the rest of the last warm-up
+            # solve as a timed step's), so the K timed steps' input copies,
+            # K solves and output copies are what it holds, the first input
+            # copy and the last output copy not overlapped with any solve
+            for t in ctxs:
+                t.wait()
+            barrier()
             t_start.record(st_k)
             streams[j ^ 1].wait_event(t_start)
         with torch.cuda.stream(st_k):
