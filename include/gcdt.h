@@ -181,7 +181,8 @@ gcdt_status gcdt_time_barriers(int device, int32_t rounds, double* us_per_barrie
    reference): on (nonzero), the stage kernel records the two read-outs
    below; off (the default), it records neither and their counters stay 0.
    The records cost a few atomics and counter updates per phase (0.5% of
-   the 10M-point solve), so timed runs leave it off.  Returns GCDT_OK. */
+   the 10M-point solve), so timed runs leave it off.  Returns GCDT_OK, or
+   GCDT_BAD_INPUT for a null ctx. */
 gcdt_status gcdt_set_profiling(gcdt_context* ctx, int32_t on);
 
 /* Per-phase profile of the last solve on ctx, if it ran with profiling on
